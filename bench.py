@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the Gaussian-mixture volume training step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config large|medium|small]
+
+Metric: fwd+bwd ms per step at 2M Gaussians x 16M points (the "large evaluation"
+configuration: clustered means, half the samples near Gaussian means).  One step is what
+the reference's training loop does per iteration on this path: build the sample index
+(build_bvh, train.py:366), forward (render, train.py:370), the masked L1 loss gradient
+(train.py:389-396) and the backward (train.py:445), all on device-resident inputs.
+
+N > 1 (torchrun): weak scaling -- every rank holds all Gaussians and its own 16M
+samples; the per-Gaussian gradients are summed with one NCCL all-reduce per step.
+
+--impl reference: the reference's evaluation formula restated on the CPU (the oracle:
+the reference's CUDA extension cannot be built -- its cuBQL/glm/Viskores sources are not
+vendored), timed on bounded samples with all host threads and extrapolated to the full
+step; rank 0 only.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gaussian-volume-compression_b200")
+sys.path.insert(0, PKG)
+
+CONFIGS = {
+    # name: (P, S, description)
+    "large": (2_000_000, 16_000_000, "large evaluation: 2M clustered Gaussians x 16M points (8M uniform + 8M near means)"),
+    "medium": (200_000, 4_000_000, "scaled large evaluation: 200k clustered Gaussians x 4M points"),
+    "small": (200_000, 2_000_000, "profiling case: 200k clustered Gaussians x 2M points"),
+}
+METRIC = "fwd+bwd ms/step (2M Gaussians×16M pts), TC vs plain FP32 at stated FP64 err"
+# Algorithmic FP32 work per pair (FORWARD forward.cu:224-256, BACKWARD backward.cu:252-298):
+F_CAND = 24            # d = x - mu, quadratic form, -0.5 (every candidate pair)
+F_FWD_CONTRIB = 28     # + w e, two accumulations (contributing pair, plus one EX2)
+F_BWD_CONTRIB = 64     # recompute + adjoint (contributing pair with W > 0.01, plus one EX2)
+EX2_EQUIV = 8          # MUFU ex2 issue cost in FP32-lane units (16/clk/SM vs 128/clk/SM)
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="large", choices=list(CONFIGS))
+    p.add_argument("--bwd-mode", default="auto", choices=["auto", "deterministic", "atomic"])
+    p.add_argument("--use-gaussian-bvh", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile", action="store_true", help="minimal run for ncu (no e2e, no CPU baseline)")
+    return p.parse_args()
+
+
+def workload(cfg, rank):
+    import gvc_workloads as wl
+    P, S, desc = CONFIGS[cfg]
+    means, scales, rots, values, weights, _ = wl.mixture_large(seed=0, P=P, S=2)
+    # per-rank sample set (weak scaling); rank 0 uses the config's own seed
+    _, _, _, _, _, samples = wl.mixture_large(seed=0 if rank == 0 else 1000 + rank, P=P, S=S)
+    return means, scales, rots, values, weights, samples, desc
+
+
+def target_field(samples_t):
+    """Synthetic target of the L1 loss (the large configuration names none)."""
+    import torch
+    x, y, z = samples_t[:, 0], samples_t[:, 1], samples_t[:, 2]
+    return 0.5 + 0.4 * torch.sin(6 * x) * torch.sin(5 * y) * torch.sin(4 * z)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained"), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+# ----------------------------------------------------------------------------------------
+# CPU baseline: the oracle (the reference formula restated in C, OpenMP) on bounded samples
+# ----------------------------------------------------------------------------------------
+def cpu_step_time(means, scales, rots, values, weights, samples, n_sub, seed=5):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    rng = np.random.default_rng(seed)
+    sub = samples[rng.choice(samples.shape[0], n_sub, replace=False)]
+    t0 = time.perf_counter()
+    c32, _, bb = oracle.preprocess(means, scales, rots, weights)
+    out, outw = oracle.forward(means, values, weights, c32.astype(np.float64), bb, sub)
+    gt = 0.5 + 0.4 * np.sin(6 * sub[:, 0]) * np.sin(5 * sub[:, 1]) * np.sin(4 * sub[:, 2])
+    mask = out != -1
+    g = np.where(mask, np.sign(out - gt), 0.0) / max(int(mask.sum()), 1)
+    r = oracle.backward(means, values, weights, c32.astype(np.float64), bb, sub, out.astype(np.float32),
+                        outw.astype(np.float32), g.astype(np.float32), np.zeros(n_sub, np.float32))
+    oracle.cov_backward(scales, rots, c32, r["dconics"])
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(means, scales, rots, values, weights, samples, sizes=(250_000, 1_000_000)):
+    """Times the oracle at two sample counts and extrapolates linearly to the full S."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.lib()
+    threads = os.cpu_count() or 1
+    t = [cpu_step_time(means, scales, rots, values, weights, samples, n) for n in sizes]
+    slope = (t[1] - t[0]) / (sizes[1] - sizes[0])
+    fixed = max(t[0] - slope * sizes[0], 0.0)
+    full = fixed + slope * samples.shape[0]
+    return {"value": full * 1e3, "unit": "ms/step", "cores": threads, "kind": "port",
+            "sample": "oracle fwd+bwd (C, OpenMP %d threads) on %d and %d of the %d points with all %d Gaussians "
+                      "(%.2f s, %.2f s), linearly extrapolated to the full step" %
+                      (threads, sizes[0], sizes[1], samples.shape[0], means.shape[0], t[0], t[1]),
+            "extrapolated": True}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    means, scales, rots, values, weights, samples, desc = workload(args.config, 0)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.lib()
+    threads = os.cpu_count() or 1
+    S = samples.shape[0]
+    n_a, n_b = 125_000, 500_000
+    t_a = cpu_step_time(means, scales, rots, values, weights, samples, n_a)
+    for _ in range(max(args.warmup - 1, 0)):
+        cpu_step_time(means, scales, rots, values, weights, samples, n_b)
+    times = [cpu_step_time(means, scales, rots, values, weights, samples, n_b, seed=10 + k) for k in range(args.steps)]
+    t_b = float(np.median(times))
+    slope = (t_b - t_a) / (n_b - n_a)
+    full_ms = (max(t_a - slope * n_a, 0.0) + slope * S) * 1e3
+    line = {"metric": METRIC, "value": full_ms, "unit": "ms/step", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "P": means.shape[0], "S": S},
+            "cpu_baseline": {"value": full_ms, "unit": "ms/step", "cores": threads, "kind": "port",
+                             "sample": "oracle fwd+bwd on %d (x1) and %d (x%d, median) of %d points, all Gaussians, "
+                                       "extrapolated linearly" % (n_a, n_b, args.steps, S)},
+            "e2e": {"value": full_ms, "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference CUDA extension is not buildable (cuBQL, glm and Viskores sources absent); "
+                    "this arm is the reference formula restated in C (oracle/gvc_oracle.c)"}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------
+# Our arm
+# ----------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import gvc_dist
+    import gvc_native
+    from bvh_diff_gaussian_rasterization import _C
+    import bvh_diff_gaussian_rasterization as R
+
+    rank, world, local = gvc_dist.init_from_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    means, scales, rots, values, weights, samples, desc = workload(args.config, rank)
+    P, S = means.shape[0], samples.shape[0]
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    d_means, d_scales, d_rots, d_values, d_weights, d_samples = map(T, (means, scales, rots, values, weights, samples))
+    d_gt = target_field(d_samples)
+    zeros_w = torch.zeros(S, device=dev)
+    ugb = bool(args.use_gaussian_bvh)
+    _C.set_backward_mode(args.bwd_mode)
+    bounds = (0.0, 0.0, 0.0, 1.0, 1.0, 1.0)
+
+    def step():
+        _C.build_bvh(d_samples, False, ugb)
+        out, outw, conics = _C.rasterize_gaussians(d_means, d_scales, d_rots, d_values, d_weights, 1.0,
+                                                   *bounds, -1.0, ugb, False)
+        # masked L1 (train.py:389-396): d|cells - gt|.mean() over the valid mask
+        mask = (out != -1) & (d_gt != -1)
+        g = torch.where(mask, torch.sign(out - d_gt), torch.zeros_like(out)) / mask.sum().clamp_min(1)
+        grads = _C.rasterize_gaussians_backward(d_means, d_scales, d_rots, conics, d_values, d_weights, out, outw,
+                                                1.0, *bounds, -1.0, g, zeros_w, ugb, False)
+        return gvc_dist.allreduce_grads(list(grads))
+
+    # pair counts of this workload (one untimed step)
+    _C.set_count_pairs(True)
+    step()
+    counts = _C.stats()
+    _C.set_count_pairs(False)
+    _C.check_status()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    _C.set_time_kernels(True)
+    launches0 = gvc_native.launch_count()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = gvc_native.launch_count() - launches0
+    kt = _C.stats()
+    _C.set_time_kernels(False)
+    _C.check_status()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop() if clocks else None
+    ms = gvc_dist.max_over_ranks(ms, dev)
+
+    # roofline of the dominant evaluation kernel
+    n_cand, n_fc, n_bc = counts["fwd_candidates"], counts["fwd_contributing"], counts["bwd_contributing"]
+    f_fwd = F_CAND * n_cand + (F_FWD_CONTRIB - F_CAND + EX2_EQUIV) * n_fc
+    f_bwd = F_CAND * n_cand + (F_BWD_CONTRIB - F_CAND + EX2_EQUIV) * n_bc
+    t_fwd = kt["fwd_kernel_ms"] / max(kt["fwd_kernel_calls"], 1)
+    t_bwd = kt["bwd_kernel_ms"] / max(kt["bwd_kernel_calls"], 1)
+    hbm, bf16, bf16s, src = measured_peaks()
+    if t_bwd >= t_fwd:
+        name, flops, t_k = "k_backward_gauss (Gaussian-owned adjoint)", f_bwd, t_bwd
+    else:
+        name, flops, t_k = "k_forward (tile traversal + evaluation)", f_fwd, t_fwd
+    achieved = flops / (t_k * 1e-3) / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                "frac": achieved / bf16, "traffic": None, "kernel": name, "kernel_ms": t_k,
+                "peak_source": "%s bf16 dense (MEASURED_PEAKS.json)" % src,
+                "fp32_simt_nominal_tflops": FP32_NOMINAL_TFLOPS,
+                "frac_of_fp32_simt_nominal": achieved / FP32_NOMINAL_TFLOPS,
+                "fwd_kernel_ms": t_fwd, "bwd_kernel_ms": t_bwd,
+                "pairs": {"candidates": n_cand, "fwd_contributing": n_fc, "bwd_contributing": n_bc},
+                "flops_per_pair": {"candidate": F_CAND, "fwd_contributing": F_FWD_CONTRIB,
+                                   "bwd_contributing": F_BWD_CONTRIB, "ex2_fp32_equiv": EX2_EQUIV}}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e and not args.profile:
+        h_samples = torch.from_numpy(samples).pin_memory()
+        h_params = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+                    for a in (means, scales, rots, values.reshape(-1, 1), weights.reshape(-1, 1))]
+        settings = R.GaussianRasterizationSettings((0, 0, 0), (1, 1, 1), 0, -1.0, 1.0, ugb, False)
+        rast = R.GaussianRasterizer(settings)
+        h2d = h_samples.numel() * 4 + sum(p.numel() * 4 for p in h_params)
+
+        def e2e_step():
+            s_d = h_samples.to(dev, non_blocking=True)
+            leaves = [p.to(dev, non_blocking=True).requires_grad_(True) for p in h_params]
+            rast.build_bvh(s_d)
+            cells, cw = rast(leaves[0], leaves[1], leaves[2], leaves[3], leaves[4])
+            gt = target_field(s_d)
+            mask = (cells != -1) & (gt != -1)
+            loss = torch.abs(cells[mask] - gt[mask]).mean()
+            loss.backward()
+            if world > 1:
+                gvc_dist.allreduce_grads([l.grad for l in leaves])
+            return loss.item()
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n_e2e = max(3, min(args.steps, 10))
+        a0.record(stream)
+        for _ in range(n_e2e):
+            e2e_step()
+        a1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = gvc_dist.max_over_ranks(a0.elapsed_time(a1) / n_e2e, dev)
+        e2e = {"value": e2e_ms, "unit": "ms/step", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4,
+               "steps": n_e2e, "path": "GaussianRasterizer (autograd) + masked L1 + loss.item()"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
+        cpu = cpu_baseline(means, scales, rots, values, weights, samples)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": ms, "unit": "ms/step", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": desc, "P": P, "S_per_gpu": S, "path": "plain FP32",
+                           "backward": args.bwd_mode, "use_gaussian_bvh": ugb,
+                           "l2": "inputs larger than L2 (samples %d MB, Gaussian records %d MB)" %
+                                 (S * 12 // 2**20, P * 80 // 2**20),
+                           "parallelism": "samples sharded per rank, NCCL all-reduce of gradients" if world > 1
+                           else "single GPU"},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
+                "gpu_launches": int(launches), "gpu_launches_per_step": launches / args.steps}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

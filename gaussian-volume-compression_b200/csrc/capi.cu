@@ -1,0 +1,544 @@
+// capi.cu -- extern "C" entry points of libgvc.so (declared in include/gvc.h).
+//
+// Host orchestration of the path that diff-gaussian-rasterization/ext.cu,
+// rasterize_points.cu and cuda_rasterizer/rasterizer_impl.cu implement in the
+// reference: stream-ordered, no per-call cudaMalloc once the context's buffers have
+// grown to the working sizes, no device synchronisation unless debug is set (the
+// reference synchronises every call through cudaMalloc/cudaFree and a D2H copy,
+// rasterizer_impl.cu:121-169).
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "lbvh.cuh"
+#include "render.cuh"
+
+using namespace gvc;
+
+static std::atomic<long long> g_launches{0};
+void gvc::note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+
+struct Scratch {
+    DevBuf gacc;       // [P][16] per-Gaussian gradient accumulators
+    DevBuf tmp_boxes;  // debug hooks / tet boxes
+    DevBuf tmp_out;
+    Lbvh dbg;          // debug LBVH
+    Lbvh msamp;        // Morton order of mesh sample points
+};
+
+Scratch* scratch_of(gvc_ctx* c);
+
+int fail(gvc_ctx* c, int code, const char* msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(gvc_ctx* c, cudaError_t e, const char* where) {
+    if (c) {
+        c->err = std::string(where) + ": " + cudaGetErrorString(e);
+    }
+    return GVC_ERR_CUDA;
+}
+
+#define GVC_CUDA(call, where)                                   \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+    } while (0)
+
+__global__ void k_boxes6_to_f4(int64_t n, const float* __restrict__ b6, float4* __restrict__ out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[2 * i] = make_float4(b6[6 * i], b6[6 * i + 1], b6[6 * i + 2], 0.f);
+    out[2 * i + 1] = make_float4(b6[6 * i + 3], b6[6 * i + 4], b6[6 * i + 5], 0.f);
+}
+
+__global__ void k_f4_to_boxes6(int64_t n, const float4* __restrict__ in, float* __restrict__ b6) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 lo = in[2 * i], hi = in[2 * i + 1];
+    b6[6 * i] = lo.x;
+    b6[6 * i + 1] = lo.y;
+    b6[6 * i + 2] = lo.z;
+    b6[6 * i + 3] = hi.x;
+    b6[6 * i + 4] = hi.y;
+    b6[6 * i + 5] = hi.z;
+}
+
+inline unsigned nb(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Largest element count handled with 32-bit indices inside the kernels.
+constexpr int64_t kMaxElems = (int64_t(1) << 31) - 4096;
+
+struct DebugTimer {
+    bool on;
+    cudaStream_t st;
+    cudaEvent_t ev[8];
+    int n = 0;
+    DebugTimer(bool on_, cudaStream_t s) : on(on_), st(s) {
+        if (on)
+            for (auto& e : ev) cudaEventCreate(&e);
+    }
+    void mark() {
+        if (on && n < 8) cudaEventRecord(ev[n++], st);
+    }
+    float ms(int a, int b) {
+        float t = 0.f;
+        if (on && b < n) cudaEventElapsedTime(&t, ev[a], ev[b]);
+        return t;
+    }
+    ~DebugTimer() {
+        if (on)
+            for (auto& e : ev) cudaEventDestroy(e);
+    }
+};
+
+// Kernel timing: events recorded around the evaluation kernels on the caller's stream;
+// read out (after a synchronisation) by gvc_get_stats or when the pool is full.
+void drain_events(gvc_ctx* ctx) {
+    for (int i = 0; i < ctx->ev_pending; i++) {
+        cudaEventSynchronize(ctx->ev_pool[2 * i + 1]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev_pool[2 * i], ctx->ev_pool[2 * i + 1]);
+        if (ctx->ev_kind[i] == 0) {
+            ctx->fwd_kernel_ms += ms;
+            ctx->fwd_kernel_calls++;
+        } else {
+            ctx->bwd_kernel_ms += ms;
+            ctx->bwd_kernel_calls++;
+        }
+    }
+    ctx->ev_pending = 0;
+}
+
+int timer_begin(gvc_ctx* ctx, cudaStream_t st, int kind) {
+    if (!ctx->time_kernels) return -1;
+    if (!ctx->ev_init) {
+        for (auto& e : ctx->ev_pool) cudaEventCreate(&e);
+        ctx->ev_init = true;
+    }
+    if (ctx->ev_pending == 32) drain_events(ctx);
+    int i = ctx->ev_pending++;
+    ctx->ev_kind[i] = kind;
+    cudaEventRecord(ctx->ev_pool[2 * i], st);
+    return i;
+}
+
+void timer_end(gvc_ctx* ctx, cudaStream_t st, int i) {
+    if (i >= 0) cudaEventRecord(ctx->ev_pool[2 * i + 1], st);
+}
+
+int debug_check(gvc_ctx* ctx, cudaStream_t st) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "debug synchronize");
+    e = cudaMemcpy(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "status copy");
+    if (*ctx->h_status & kStatusStackOverflow) {
+        cudaMemset(ctx->d_status, 0, sizeof(int));
+        return fail(ctx, GVC_ERR_TRAVERSAL, "BVH traversal stack overflow: results are invalid");
+    }
+    return GVC_OK;
+}
+
+}  // namespace
+
+struct gvc_ctx_full : gvc_ctx {
+    Scratch scratch;
+};
+
+namespace {
+Scratch* scratch_of(gvc_ctx* c) { return &static_cast<gvc_ctx_full*>(c)->scratch; }
+}  // namespace
+
+extern "C" {
+
+int64_t gvc_launch_count(void) { return (int64_t)g_launches.load(std::memory_order_relaxed); }
+
+int gvc_ctx_create(gvc_ctx** out) {
+    if (!out) return GVC_ERR_ARG;
+    *out = nullptr;
+    gvc_ctx_full* c = new (std::nothrow) gvc_ctx_full();
+    if (!c) return GVC_ERR_CAPACITY;
+    gvc_ctx* ctx = c;
+    GVC_CUDA(cudaGetDevice(&c->device), "cudaGetDevice");
+    GVC_CUDA(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc status");
+    GVC_CUDA(cudaMemset(c->d_status, 0, sizeof(int)), "cudaMemset status");
+    GVC_CUDA(cudaMalloc(&c->d_stats, sizeof(unsigned long long) * 8), "cudaMalloc stats");
+    GVC_CUDA(cudaMemset(c->d_stats, 0, sizeof(unsigned long long) * 8), "cudaMemset stats");
+    GVC_CUDA(cudaMallocHost(&c->h_status, sizeof(int)), "cudaMallocHost");
+    *out = c;
+    return GVC_OK;
+}
+
+void gvc_ctx_destroy(gvc_ctx* ctx) {
+    if (!ctx) return;
+    gvc_ctx_full* c = static_cast<gvc_ctx_full*>(ctx);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(c->device);
+    Lbvh* lbvhs[] = {&c->s_sort, &c->tiles, &c->gbvh, &c->cells, &c->scratch.dbg, &c->scratch.msamp};
+    for (Lbvh* L : lbvhs) {
+        DevBuf* bufs[] = {&L->keys, &L->keys_alt, &L->perm, &L->perm_alt, &L->boxes, &L->sorted_boxes, &L->left,
+                          &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds};
+        for (DevBuf* b : bufs) b->release();
+    }
+    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->s_grad, &c->grec, &c->gtmp,
+                      &c->m_out_sorted, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
+    for (DevBuf* b : bufs) b->release();
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->d_stats) cudaFree(c->d_stats);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->ev_init)
+        for (auto& e : c->ev_pool) cudaEventDestroy(e);
+    cudaSetDevice(prev);
+    delete c;
+}
+
+const char* gvc_last_error(const gvc_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int gvc_set_option(gvc_ctx* ctx, int option, int value) {
+    if (!ctx) return GVC_ERR_ARG;
+    switch (option) {
+        case GVC_OPT_COV_GRAD:
+            if (value < 0 || value > 1) return fail(ctx, GVC_ERR_ARG, "cov_grad must be 0 or 1");
+            ctx->cov_grad_mode = value;
+            return GVC_OK;
+        case GVC_OPT_BWD_MODE:
+            if (value < 0 || value > 2) return fail(ctx, GVC_ERR_ARG, "bwd_mode must be 0, 1 or 2");
+            ctx->bwd_mode = value;
+            return GVC_OK;
+        case GVC_OPT_EVAL_PATH:
+            if (value != 0) return fail(ctx, GVC_ERR_UNSUPPORTED, "only the plain FP32 exponent path is built");
+            ctx->eval_path = value;
+            return GVC_OK;
+        case GVC_OPT_COUNT_PAIRS:
+            ctx->count_pairs = value ? 1 : 0;
+            return GVC_OK;
+        case GVC_OPT_TIME_KERNELS:
+            drain_events(ctx);
+            ctx->time_kernels = value ? 1 : 0;
+            ctx->fwd_kernel_ms = ctx->bwd_kernel_ms = 0.0;
+            ctx->fwd_kernel_calls = ctx->bwd_kernel_calls = 0;
+            return GVC_OK;
+        default:
+            return fail(ctx, GVC_ERR_ARG, "unknown option");
+    }
+}
+
+int gvc_get_stats(gvc_ctx* ctx, gvc_stats* out, void* stream) {
+    if (!ctx || !out) return GVC_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long h[8];
+    GVC_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    GVC_CUDA(cudaMemcpy(h, ctx->d_stats, sizeof(h), cudaMemcpyDeviceToHost), "stats copy");
+    out->fwd_candidates = (int64_t)h[0];
+    out->fwd_contributing = (int64_t)h[1];
+    out->bwd_contributing = (int64_t)h[2];
+    out->max_stack_fwd = (int32_t)h[3];
+    out->max_stack_bwd = (int32_t)h[4];
+    drain_events(ctx);
+    out->fwd_kernel_ms = ctx->fwd_kernel_ms;
+    out->bwd_kernel_ms = ctx->bwd_kernel_ms;
+    out->fwd_kernel_calls = ctx->fwd_kernel_calls;
+    out->bwd_kernel_calls = ctx->bwd_kernel_calls;
+    return GVC_OK;
+}
+
+int gvc_sync_status(gvc_ctx* ctx, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    return debug_check(ctx, (cudaStream_t)stream);
+}
+
+int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int use_gaussian_bvh, void* stream) {
+    (void)use_gaussian_bvh;  // both reference modes use the same sample ordering here
+    if (!ctx) return GVC_ERR_ARG;
+    if (S < 0 || S > kMaxElems) return fail(ctx, GVC_ERR_CAPACITY, "number of samples out of range");
+    if (S > 0 && !samples) return fail(ctx, GVC_ERR_ARG, "samples is null");
+    cudaStream_t st = (cudaStream_t)stream;
+    DebugTimer tm(debug != 0, st);
+    tm.mark();
+    ctx->samples = samples;
+    ctx->S = S;
+    ctx->n_tiles = (S + kTile - 1) / kTile;
+    ctx->samples_ready = false;
+    if (S > 0) {
+        GVC_CUDA(morton_sort_points(ctx->s_sort, S, samples, st), "sample sort");
+        const int64_t slots = ctx->n_tiles * kTile;
+        GVC_CUDA(ctx->s_sorted.ensure(sizeof(float4) * slots), "alloc s_sorted");
+        GVC_CUDA(ctx->tile_boxes.ensure(sizeof(float4) * 2 * ctx->n_tiles), "alloc tile_boxes");
+        GVC_CUDA(ctx->tile_keys.ensure(sizeof(uint32_t) * ctx->n_tiles), "alloc tile_keys");
+        GVC_CUDA(launch_sample_tiles(S, ctx->n_tiles, samples, ctx->s_sort.perm.as<int32_t>(),
+                                     ctx->s_sort.keys.as<uint32_t>(), ctx->s_sorted.as<float4>(),
+                                     ctx->tile_boxes.as<float4>(), ctx->tile_keys.as<uint32_t>(), st),
+                 "sample tiles");
+        GVC_CUDA(lbvh_hierarchy(ctx->tiles, ctx->n_tiles, ctx->tile_keys.as<uint32_t>(),
+                                ctx->tile_boxes.as<float4>(), st),
+                 "tile LBVH");
+    }
+    ctx->samples_ready = true;
+    tm.mark();
+    if (debug) {
+        int rc = debug_check(ctx, st);
+        printf("Sample BVH time: %g ms\n", tm.ms(0, 1));
+        if (rc) return rc;
+    }
+    return GVC_OK;
+}
+
+int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const float* scales,
+                            const float* rotations, const float* values, const float* weights, float scale_modifier,
+                            const float* bounds, float bg, int use_gaussian_bvh, int debug, float* out_cells,
+                            float* out_weights, float* conics, void* stream) {
+    (void)bounds;
+    (void)bg;
+    (void)use_gaussian_bvh;
+    if (!ctx) return GVC_ERR_ARG;
+    if (!ctx->samples_ready) return fail(ctx, GVC_ERR_STATE, "build_bvh must be called before rasterize_gaussians");
+    if (P < 0 || P > kMaxElems) return fail(ctx, GVC_ERR_CAPACITY, "number of Gaussians out of range");
+    const int64_t S = ctx->S;
+    if (S > 0 && (!out_cells || !out_weights)) return fail(ctx, GVC_ERR_ARG, "null output");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (P == 0) {  // rasterize_points.cu:51: outputs stay zero
+        GVC_CUDA(launch_fill_zero_outputs(S, out_cells, out_weights, st), "zero outputs");
+        ctx->gauss_ready = false;
+        return GVC_OK;
+    }
+    if (!means3D || !scales || !rotations || !values || !weights || !conics)
+        return fail(ctx, GVC_ERR_ARG, "null Gaussian parameter pointer");
+    DebugTimer tm(debug != 0, st);
+    if (ctx->count_pairs) GVC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, sizeof(unsigned long long) * 8, st), "stats");
+    tm.mark();
+    GVC_CUDA(ctx->gtmp.ensure(sizeof(float4) * 2 * P), "alloc boxes");
+    float4* boxes = ctx->gtmp.as<float4>();
+    GVC_CUDA(launch_preprocess(P, means3D, scales, rotations, weights, scale_modifier, conics, boxes, st),
+             "preprocess");
+    tm.mark();
+    GVC_CUDA(lbvh_build_boxes(ctx->gbvh, P, boxes, st), "Gaussian LBVH");
+    GVC_CUDA(ctx->grec.ensure(sizeof(GaussRec) * P), "alloc records");
+    GVC_CUDA(launch_gather_recs(P, ctx->gbvh.perm.as<int32_t>(), means3D, values, weights, conics, boxes,
+                                ctx->grec.as<GaussRec>(), st),
+             "gather records");
+    tm.mark();
+    FwdArgs fa;
+    fa.s_sorted = ctx->s_sorted.as<float4>();
+    fa.tile_boxes = ctx->tile_boxes.as<float4>();
+    fa.n_tiles = ctx->n_tiles;
+    fa.gnodes = ctx->gbvh.nodes.as<BvhNode>();
+    fa.recs = ctx->grec.as<GaussRec>();
+    fa.out_cells = out_cells;
+    fa.out_weights = out_weights;
+    fa.status = ctx->d_status;
+    fa.stats = ctx->d_stats;
+    fa.count = ctx->count_pairs != 0;
+    const int tk = timer_begin(ctx, st, 0);
+    GVC_CUDA(launch_forward(fa, st), "forward");
+    timer_end(ctx, st, tk);
+    tm.mark();
+    ctx->P = P;
+    ctx->gauss_ready = true;
+    if (debug) {
+        int rc = debug_check(ctx, st);
+        printf("Preprocess time: %g ms\nBVH time: %g ms\nRender time: %g ms\n", tm.ms(0, 1), tm.ms(1, 2),
+               tm.ms(2, 3));
+        if (rc) return rc;
+    }
+    return GVC_OK;
+}
+
+int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means3D, const float* scales,
+                                     const float* rotations, const float* conics, const float* values,
+                                     const float* weights, const float* out_cells, const float* out_weights,
+                                     float scale_modifier, const float* bounds, float bg, const float* dL_dout_cells,
+                                     const float* dL_dout_weights, int use_gaussian_bvh, int debug, float* dmeans,
+                                     float* dscales, float* drots, float* dvalues, float* dweights, void* stream) {
+    (void)bounds;
+    (void)bg;
+    if (!ctx) return GVC_ERR_ARG;
+    if (!ctx->samples_ready)
+        return fail(ctx, GVC_ERR_STATE, "build_bvh must be called before rasterize_gaussians_backward");
+    if (P < 0 || P > kMaxElems) return fail(ctx, GVC_ERR_CAPACITY, "number of Gaussians out of range");
+    if (P == 0) return GVC_OK;
+    if (!means3D || !scales || !rotations || !conics || !values || !weights || !dmeans || !dscales || !drots ||
+        !dvalues || !dweights)
+        return fail(ctx, GVC_ERR_ARG, "null pointer");
+    const int64_t S = ctx->S;
+    if (S > 0 && (!out_cells || !out_weights || !dL_dout_cells || !dL_dout_weights))
+        return fail(ctx, GVC_ERR_ARG, "null sample-side pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch* sc = scratch_of(ctx);
+    DebugTimer tm(debug != 0, st);
+    tm.mark();
+    GVC_CUDA(ctx->gtmp.ensure(sizeof(float4) * 2 * P), "alloc boxes");
+    float4* boxes = ctx->gtmp.as<float4>();
+    GVC_CUDA(launch_preprocess(P, means3D, scales, rotations, weights, scale_modifier, nullptr, boxes, st),
+             "preprocess");
+    GVC_CUDA(sc->gacc.ensure(sizeof(float) * 16 * P), "alloc gacc");
+    float* gacc = sc->gacc.as<float>();
+    const bool atomic_mode = ctx->bwd_mode == 2 || (ctx->bwd_mode == 0 && use_gaussian_bvh);
+    const bool have_order = ctx->gauss_ready && ctx->P == P;
+    if (ctx->n_tiles == 0) {
+        GVC_CUDA(cudaMemsetAsync(gacc, 0, sizeof(float) * 16 * P, st), "zero gacc");
+    } else {
+        const int64_t slots = ctx->n_tiles * kTile;
+        GVC_CUDA(ctx->s_grad.ensure(sizeof(float4) * slots), "alloc s_grad");
+        GVC_CUDA(launch_sample_grads(slots, ctx->s_sorted.as<float4>(), out_cells, out_weights, dL_dout_cells,
+                                     dL_dout_weights, ctx->s_grad.as<float4>(), st),
+                 "sample grads");
+        BwdArgs ba;
+        ba.P = P;
+        ba.means = means3D;
+        ba.values = values;
+        ba.weights = weights;
+        ba.conics = conics;
+        ba.boxes = boxes;
+        ba.s_sorted = ctx->s_sorted.as<float4>();
+        ba.s_grad = ctx->s_grad.as<float4>();
+        ba.tile_boxes = ctx->tile_boxes.as<float4>();
+        ba.n_tiles = ctx->n_tiles;
+        ba.tnodes = ctx->tiles.nodes.as<BvhNode>();
+        ba.gacc = gacc;
+        ba.status = ctx->d_status;
+        ba.stats = ctx->d_stats;
+        ba.count = ctx->count_pairs != 0;
+        tm.mark();
+        if (atomic_mode) {
+            if (!have_order) GVC_CUDA(lbvh_build_boxes(ctx->gbvh, P, boxes, st), "Gaussian LBVH");
+            GVC_CUDA(ctx->grec.ensure(sizeof(GaussRec) * P), "alloc records");
+            GVC_CUDA(launch_gather_recs(P, ctx->gbvh.perm.as<int32_t>(), means3D, values, weights, conics, boxes,
+                                        ctx->grec.as<GaussRec>(), st),
+                     "gather records");
+            GVC_CUDA(cudaMemsetAsync(gacc, 0, sizeof(float) * 16 * P, st), "zero gacc");
+            ba.gorder = nullptr;
+            ba.gperm = ctx->gbvh.perm.as<int32_t>();
+            ba.gnodes = ctx->gbvh.nodes.as<BvhNode>();
+            ba.recs = ctx->grec.as<GaussRec>();
+            const int tk = timer_begin(ctx, st, 1);
+            GVC_CUDA(launch_backward_tiles(ba, st), "backward (atomic)");
+            timer_end(ctx, st, tk);
+        } else {
+            ba.gorder = have_order ? ctx->gbvh.perm.as<int32_t>() : nullptr;
+            ba.gperm = nullptr;
+            ba.gnodes = nullptr;
+            ba.recs = nullptr;
+            const int tk = timer_begin(ctx, st, 1);
+            GVC_CUDA(launch_backward_gauss(ba, st), "backward (deterministic)");
+            timer_end(ctx, st, tk);
+        }
+    }
+    tm.mark();
+    GVC_CUDA(launch_finalize(P, gacc, scales, rotations, conics, scale_modifier, ctx->cov_grad_mode, dmeans, dscales,
+                             drots, dvalues, dweights, st),
+             "finalize");
+    tm.mark();
+    if (debug) {
+        int rc = debug_check(ctx, st);
+        printf("Backward render time: %g ms\nBackward preprocess time: %g ms\n", tm.ms(1, 2), tm.ms(2, 3));
+        if (rc) return rc;
+    }
+    return GVC_OK;
+}
+
+int gvc_sample_uniform(gvc_ctx* ctx, const int64_t* dims, const float* origin, const float* spacing,
+                       const void* values, int dtype, int64_t N, const float* samples, void* out, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (!dims || !origin || !spacing) return fail(ctx, GVC_ERR_ARG, "dims/origin/spacing must be host arrays");
+    if (dtype < GVC_F64 || dtype > GVC_U8)
+        return fail(ctx, GVC_ERR_UNSUPPORTED, "Unsupported values dtype. Expected float64, float32, uint16, or uint8.");
+    for (int a = 0; a < 3; a++)
+        if (dims[a] < 1) return fail(ctx, GVC_ERR_ARG, "dims must be >= 1");
+    if (N < 0) return fail(ctx, GVC_ERR_ARG, "negative sample count");
+    if (N > 0 && (!values || !samples || !out)) return fail(ctx, GVC_ERR_ARG, "null pointer");
+    GVC_CUDA(launch_sample_uniform(dims, origin, spacing, values, dtype, N, samples, out, (cudaStream_t)stream),
+             "sample_uniform");
+    return GVC_OK;
+}
+
+int gvc_sample_tets(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, const int32_t* conn4,
+                    const double* values, int64_t N, const float* samples, double* out, int64_t* cell_ids,
+                    void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (npts < 0 || C < 0 || N < 0) return fail(ctx, GVC_ERR_ARG, "negative size");
+    if (C > kMaxElems || N > kMaxElems) return fail(ctx, GVC_ERR_CAPACITY, "mesh or sample count out of range");
+    if (N > 0 && (!samples || !out)) return fail(ctx, GVC_ERR_ARG, "null pointer");
+    if (C > 0 && (!pts || !conn4 || !values)) return fail(ctx, GVC_ERR_ARG, "null mesh pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch* sc = scratch_of(ctx);
+    if (N == 0) return GVC_OK;
+    const int32_t* cperm = nullptr;
+    const BvhNode* cnodes = nullptr;
+    if (C > 0) {
+        GVC_CUDA(sc->tmp_boxes.ensure(sizeof(float4) * 2 * C), "alloc cell boxes");
+        GVC_CUDA(launch_tet_boxes(C, pts, conn4, sc->tmp_boxes.as<float4>(), st), "tet boxes");
+        GVC_CUDA(lbvh_build_boxes(ctx->cells, C, sc->tmp_boxes.as<float4>(), st), "cell LBVH");
+        cperm = ctx->cells.perm.as<int32_t>();
+        cnodes = ctx->cells.nodes.as<BvhNode>();
+    }
+    GVC_CUDA(morton_sort_points(sc->msamp, N, samples, st), "sample order");
+    GVC_CUDA(launch_sample_tets(N, samples, sc->msamp.perm.as<int32_t>(), pts, conn4, values, cnodes, cperm, C, out,
+                                cell_ids, ctx->d_status, st),
+             "sample tets");
+    return GVC_OK;
+}
+
+int gvc_debug_lbvh(gvc_ctx* ctx, int64_t n, const float* boxes, uint32_t* keys_sorted, int32_t* perm,
+                   int32_t* left, int32_t* right, float* node_boxes, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (n <= 0 || n > kMaxElems) return fail(ctx, GVC_ERR_ARG, "n out of range");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch* sc = scratch_of(ctx);
+    GVC_CUDA(sc->tmp_boxes.ensure(sizeof(float4) * 2 * n), "alloc");
+    k_boxes6_to_f4<<<nb(n, 256), 256, 0, st>>>(n, boxes, sc->tmp_boxes.as<float4>()); gvc::note_launch();
+    GVC_CUDA(lbvh_build_boxes(sc->dbg, n, sc->tmp_boxes.as<float4>(), st), "LBVH");
+    if (keys_sorted)
+        GVC_CUDA(cudaMemcpyAsync(keys_sorted, sc->dbg.keys.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st),
+                 "copy keys");
+    if (perm)
+        GVC_CUDA(cudaMemcpyAsync(perm, sc->dbg.perm.ptr, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st),
+                 "copy perm");
+    if (n > 1) {
+        if (left)
+            GVC_CUDA(cudaMemcpyAsync(left, sc->dbg.left.ptr, sizeof(int32_t) * (n - 1), cudaMemcpyDeviceToDevice, st),
+                     "copy left");
+        if (right)
+            GVC_CUDA(
+                cudaMemcpyAsync(right, sc->dbg.right.ptr, sizeof(int32_t) * (n - 1), cudaMemcpyDeviceToDevice, st),
+                "copy right");
+        if (node_boxes) k_f4_to_boxes6<<<nb(n - 1, 256), 256, 0, st>>>(n - 1, sc->dbg.node_boxes.as<float4>(), node_boxes); gvc::note_launch();
+    }
+    GVC_CUDA(cudaGetLastError(), "debug lbvh");
+    return GVC_OK;
+}
+
+int gvc_debug_preprocess(gvc_ctx* ctx, int64_t P, const float* means3D, const float* scales, const float* rotations,
+                         const float* weights, float scale_modifier, float* conics, float* aabbs, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (P <= 0 || P > kMaxElems) return fail(ctx, GVC_ERR_ARG, "P out of range");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch* sc = scratch_of(ctx);
+    GVC_CUDA(sc->tmp_boxes.ensure(sizeof(float4) * 2 * P), "alloc");
+    GVC_CUDA(launch_preprocess(P, means3D, scales, rotations, weights, scale_modifier, conics,
+                               sc->tmp_boxes.as<float4>(), st),
+             "preprocess");
+    if (aabbs) k_f4_to_boxes6<<<nb(P, 256), 256, 0, st>>>(P, sc->tmp_boxes.as<float4>(), aabbs); gvc::note_launch();
+    GVC_CUDA(cudaGetLastError(), "debug preprocess");
+    return GVC_OK;
+}
+
+int gvc_debug_sample_order(gvc_ctx* ctx, int32_t* perm, uint32_t* keys, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (!ctx->samples_ready) return fail(ctx, GVC_ERR_STATE, "no samples");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ctx->S == 0) return GVC_OK;
+    if (perm)
+        GVC_CUDA(cudaMemcpyAsync(perm, ctx->s_sort.perm.ptr, sizeof(int32_t) * ctx->S, cudaMemcpyDeviceToDevice, st),
+                 "copy perm");
+    if (keys)
+        GVC_CUDA(cudaMemcpyAsync(keys, ctx->s_sort.keys.ptr, sizeof(uint32_t) * ctx->S, cudaMemcpyDeviceToDevice, st),
+                 "copy keys");
+    return GVC_OK;
+}
+
+}  // extern "C"

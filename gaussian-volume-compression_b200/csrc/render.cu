@@ -1,0 +1,524 @@
+// render.cu -- fused traversal + Gaussian evaluation (forward) and the adjoint
+// (backward) of the mixture field at Morton-sorted sample tiles.
+//
+// Forward (replaces FORWARD::sampleRenderCUDA / renderCUDA + normalizeCUDA,
+// diff-gaussian-rasterization/cuda_rasterizer/forward.cu:116-274): one warp per tile of
+// 32 Morton-sorted samples walks the Gaussian LBVH with the tile's box; candidate
+// Gaussians are staged 32 at a time in shared memory and every lane evaluates its own
+// sample against each of them, accumulating W and V in registers (no atomics).
+//
+// Backward, deterministic (replaces BACKWARD::renderCUDA, backward.cu:127-337): one
+// warp per Gaussian walks the sample-tile LBVH with the Gaussian's AABB; lanes are the
+// tile's samples; per-lane partial sums are reduced once per Gaussian (a fixed-order
+// segmented reduction, no atomics).
+//
+// Backward, atomic (replaces BACKWARD::sampleRenderCUDA, backward.cu:339-559): one warp
+// per sample tile re-walks the Gaussian LBVH; the 11 per-pair terms are pre-reduced over
+// the tile with 16 shuffles and added with one FP32 atomic per field and Gaussian.
+//
+// Pair math follows forward.cu:224-256 and backward.cu:252-298; the per-sample factors
+// 1/W, -out/W are folded into the sample record once per sample.
+#include "render.cuh"
+#include "traverse.cuh"
+
+namespace gvc {
+
+constexpr int kWarpsPerBlock = 4;
+
+// --------------------------------------------------------------------------------
+// Forward
+// --------------------------------------------------------------------------------
+struct FwdVisitor {
+    const GaussRec* __restrict__ recs;
+    float4* batch;  // shared [32 * 5]
+    float x, y, z;
+    bool valid;
+    float W, V;
+    int ncand, ncontrib;
+
+    __device__ __forceinline__ void operator()(const int* c, int nb) {
+        const int lane = threadIdx.x & 31;
+        if (lane < nb) {
+            const float4* rp = reinterpret_cast<const float4*>(recs + c[lane]);
+            float4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2), r3 = __ldg(rp + 3), r4 = __ldg(rp + 4);
+            batch[lane * 5 + 0] = r0;
+            batch[lane * 5 + 1] = r1;
+            batch[lane * 5 + 2] = r2;
+            batch[lane * 5 + 3] = r3;
+            batch[lane * 5 + 4] = r4;
+        }
+        __syncwarp();
+        if (valid) {
+            for (int g = 0; g < nb; g++) {
+                const float4 r3 = batch[g * 5 + 3], r4 = batch[g * 5 + 4];
+                if (!(r3.x <= x && x <= r4.x && r3.y <= y && y <= r4.y && r3.z <= z && z <= r4.z)) continue;
+                const float4 r0 = batch[g * 5 + 0], r1 = batch[g * 5 + 1], r2 = batch[g * 5 + 2];
+                ncand++;
+                const float dx = x - r0.x, dy = y - r0.y, dz = z - r0.z;
+                const float q = dx * (r1.x * dx + r1.y * dy + r1.z * dz) + dy * (r1.y * dx + r1.w * dy + r2.x * dz) +
+                                dz * (r1.z * dx + r2.x * dy + r2.y * dz);
+                const float p = -0.5f * q;
+                if (p < kPowerFloor || p > 0.0f) continue;
+                const float wt = r0.w * __expf(p);
+                W += wt;
+                V += wt * r2.z;
+                ncontrib++;
+            }
+        }
+        __syncwarp();
+    }
+};
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_forward(const float4* __restrict__ s_sorted,
+                                                                 const float4* __restrict__ tile_boxes, int n_tiles,
+                                                                 const BvhNode* __restrict__ nodes,
+                                                                 const GaussRec* __restrict__ recs,
+                                                                 float* __restrict__ out_cells,
+                                                                 float* __restrict__ out_weights, int* status,
+                                                                 unsigned long long* stats) {
+    __shared__ int s_stack[kWarpsPerBlock][kStackCap];
+    __shared__ int s_cand[kWarpsPerBlock][kCandCap];
+    __shared__ float4 s_batch[kWarpsPerBlock][32 * 5];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x * kWarpsPerBlock + warp;
+    if (tile >= n_tiles) return;
+    const float4 sp = s_sorted[(int64_t)tile * 32 + lane];
+    const int orig = __float_as_int(sp.w);
+    FwdVisitor vis{recs, s_batch[warp], sp.x, sp.y, sp.z, orig >= 0, 0.f, 0.f, 0, 0};
+    const float4 tlo = tile_boxes[2 * (int64_t)tile], thi = tile_boxes[2 * (int64_t)tile + 1];
+    int max_sp = 0;
+    const int st = warp_traverse(nodes, make_float3(tlo.x, tlo.y, tlo.z), make_float3(thi.x, thi.y, thi.z),
+                                 s_stack[warp], s_cand[warp], vis, max_sp);
+    if (orig >= 0) {
+        float o, w;
+        if (vis.W <= kWeightCutoff) {
+            o = -1.0f;
+            w = 0.0f;
+        } else {
+            o = vis.V / vis.W;
+            w = vis.W;
+        }
+        out_cells[orig] = o;
+        out_weights[orig] = w;
+    }
+    if (st && lane == 0) atomicOr(status, st);
+    if (COUNT) {
+        unsigned long long a = (unsigned long long)vis.ncand, b = (unsigned long long)vis.ncontrib;
+        for (int off = 16; off > 0; off >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, off);
+            b += __shfl_xor_sync(0xffffffffu, b, off);
+        }
+        if (lane == 0) {
+            atomicAdd(&stats[0], a);
+            atomicAdd(&stats[1], b);
+            atomicMax(&stats[3], (unsigned long long)max_sp);
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------
+// Backward helpers: the per-pair adjoint of one (sample, Gaussian) pair.
+//   sample grad record sg = (gO/W, -gO*out/W, gW, ok) with ok = 1 iff W > 0.01.
+//   acc: 0 dv, 1 dw, 2..4 dmean, 5..10 dconic (unique parameters, off-diagonals x2).
+// --------------------------------------------------------------------------------
+struct GaussParams {
+    float mx, my, mz, w, v;
+    float c0, c1, c2, c3, c4, c5;
+    float4 lo, hi;
+};
+
+__device__ __forceinline__ bool pair_adjoint(const GaussParams& g, float4 sp, float4 sg, float (&acc)[16]) {
+    if (!(g.lo.x <= sp.x && sp.x <= g.hi.x && g.lo.y <= sp.y && sp.y <= g.hi.y && g.lo.z <= sp.z && sp.z <= g.hi.z))
+        return false;
+    if (sg.w == 0.0f) return false;
+    const float dx = sp.x - g.mx, dy = sp.y - g.my, dz = sp.z - g.mz;
+    const float t0 = g.c0 * dx + g.c1 * dy + g.c2 * dz;
+    const float t1 = g.c1 * dx + g.c3 * dy + g.c4 * dz;
+    const float t2 = g.c2 * dx + g.c4 * dy + g.c5 * dz;
+    const float p = -0.5f * (dx * t0 + dy * t1 + dz * t2);
+    if (p < kPowerFloor || p > 0.0f) return false;
+    const float e = __expf(p);
+    const float wt = g.w * e;
+    acc[0] += sg.x * wt;                       // dL/dv = gO * wt / W
+    const float gsum = g.v * sg.x + sg.y + sg.z;  // gO (v - out) / W + gW
+    acc[1] += gsum * e;                        // dL/dw
+    const float gw = gsum * wt;                // = -2 dL/dquad
+    acc[2] += gw * t0;
+    acc[3] += gw * t1;
+    acc[4] += gw * t2;
+    const float dq = -0.5f * gw;               // dL/dquad
+    acc[5] += dq * dx * dx;
+    acc[6] += dq * 2.0f * dx * dy;
+    acc[7] += dq * 2.0f * dx * dz;
+    acc[8] += dq * dy * dy;
+    acc[9] += dq * 2.0f * dy * dz;
+    acc[10] += dq * dz * dz;
+    return true;
+}
+
+// --------------------------------------------------------------------------------
+// Backward, deterministic Gaussian-owned segmented reduction.
+// --------------------------------------------------------------------------------
+struct BwdGaussVisitor {
+    const float4* __restrict__ s_sorted;
+    const float4* __restrict__ s_grad;
+    GaussParams g;
+    float acc[16];
+    int npairs;
+
+    __device__ __forceinline__ void operator()(const int* c, int nb) {
+        const int lane = threadIdx.x & 31;
+        int64_t t = c[0];
+        float4 sp = __ldg(s_sorted + t * 32 + lane), sg = __ldg(s_grad + t * 32 + lane);
+        for (int i = 0; i < nb; i++) {
+            const float4 cs = sp, cg = sg;
+            if (i + 1 < nb) {
+                t = c[i + 1];
+                sp = __ldg(s_sorted + t * 32 + lane);
+                sg = __ldg(s_grad + t * 32 + lane);
+            }
+            npairs += pair_adjoint(g, cs, cg, acc) ? 1 : 0;
+        }
+        __syncwarp();
+    }
+};
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_gauss(
+    int P, const int32_t* __restrict__ gorder, const float* __restrict__ means, const float* __restrict__ values,
+    const float* __restrict__ weights, const float* __restrict__ conics, const float4* __restrict__ boxes,
+    const float4* __restrict__ s_sorted, const float4* __restrict__ s_grad, const BvhNode* __restrict__ tnodes,
+    float* __restrict__ gacc, int* status, unsigned long long* stats) {
+    __shared__ int s_stack[kWarpsPerBlock][kStackCap];
+    __shared__ int s_cand[kWarpsPerBlock][kCandCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gi = blockIdx.x * kWarpsPerBlock + warp;
+    if (gi >= P) return;
+    const int o = gorder ? gorder[gi] : gi;
+    BwdGaussVisitor vis;
+    vis.s_sorted = s_sorted;
+    vis.s_grad = s_grad;
+    vis.g.mx = __ldg(means + 3 * (int64_t)o);
+    vis.g.my = __ldg(means + 3 * (int64_t)o + 1);
+    vis.g.mz = __ldg(means + 3 * (int64_t)o + 2);
+    vis.g.w = __ldg(weights + o);
+    vis.g.v = __ldg(values + o);
+    vis.g.c0 = __ldg(conics + 6 * (int64_t)o);
+    vis.g.c1 = __ldg(conics + 6 * (int64_t)o + 1);
+    vis.g.c2 = __ldg(conics + 6 * (int64_t)o + 2);
+    vis.g.c3 = __ldg(conics + 6 * (int64_t)o + 3);
+    vis.g.c4 = __ldg(conics + 6 * (int64_t)o + 4);
+    vis.g.c5 = __ldg(conics + 6 * (int64_t)o + 5);
+    vis.g.lo = __ldg(boxes + 2 * (int64_t)o);
+    vis.g.hi = __ldg(boxes + 2 * (int64_t)o + 1);
+#pragma unroll
+    for (int k = 0; k < 16; k++) vis.acc[k] = 0.f;
+    vis.npairs = 0;
+    int max_sp = 0;
+    const int st = warp_traverse(tnodes, make_float3(vis.g.lo.x, vis.g.lo.y, vis.g.lo.z),
+                                 make_float3(vis.g.hi.x, vis.g.hi.y, vis.g.hi.z), s_stack[warp], s_cand[warp], vis,
+                                 max_sp);
+    const float tot = warp_transpose_reduce16(vis.acc);
+    if (!(lane & 1)) {
+        const int k = lane >> 1;  // value index held by this lane
+        gacc[16 * (int64_t)o + k] = tot;
+    }
+    if (st && lane == 0) atomicOr(status, st);
+    if (COUNT) {
+        unsigned long long a = (unsigned long long)vis.npairs;
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+        if (lane == 0) {
+            atomicAdd(&stats[2], a);
+            atomicMax(&stats[4], (unsigned long long)max_sp);
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------
+// Backward, sample-tile traversal with warp pre-reduction + FP32 atomics.
+// --------------------------------------------------------------------------------
+struct BwdTileVisitor {
+    const GaussRec* __restrict__ recs;
+    const int32_t* __restrict__ gperm;
+    float4* batch;  // shared [32 * 5]
+    float4 sp, sg;
+    float* __restrict__ gacc;
+    int npairs;
+
+    __device__ __forceinline__ void operator()(const int* c, int nb) {
+        const int lane = threadIdx.x & 31;
+        if (lane < nb) {
+            const float4* rp = reinterpret_cast<const float4*>(recs + c[lane]);
+            batch[lane * 5 + 0] = __ldg(rp);
+            batch[lane * 5 + 1] = __ldg(rp + 1);
+            batch[lane * 5 + 2] = __ldg(rp + 2);
+            batch[lane * 5 + 3] = __ldg(rp + 3);
+            batch[lane * 5 + 4] = __ldg(rp + 4);
+        }
+        __syncwarp();
+        for (int gi = 0; gi < nb; gi++) {
+            const float4 r0 = batch[gi * 5 + 0], r1 = batch[gi * 5 + 1], r2 = batch[gi * 5 + 2];
+            GaussParams g;
+            g.mx = r0.x; g.my = r0.y; g.mz = r0.z; g.w = r0.w;
+            g.c0 = r1.x; g.c1 = r1.y; g.c2 = r1.z; g.c3 = r1.w;
+            g.c4 = r2.x; g.c5 = r2.y; g.v = r2.z;
+            g.lo = batch[gi * 5 + 3];
+            g.hi = batch[gi * 5 + 4];
+            float acc[16];
+#pragma unroll
+            for (int k = 0; k < 16; k++) acc[k] = 0.f;
+            const bool hit = pair_adjoint(g, sp, sg, acc);
+            const uint32_t any = __ballot_sync(0xffffffffu, hit);
+            if (any == 0u) continue;
+            npairs += hit ? 1 : 0;
+            const float tot = warp_transpose_reduce16(acc);
+            const int k = lane >> 1;
+            if (!(lane & 1) && k < 11) {
+                const int o = gperm[c[gi]];
+                atomicAdd(gacc + 16 * (int64_t)o + k, tot);
+            }
+        }
+        __syncwarp();
+    }
+};
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_tiles(
+    const float4* __restrict__ s_sorted, const float4* __restrict__ s_grad, const float4* __restrict__ tile_boxes,
+    int n_tiles, const BvhNode* __restrict__ gnodes, const GaussRec* __restrict__ recs,
+    const int32_t* __restrict__ gperm, float* __restrict__ gacc, int* status, unsigned long long* stats) {
+    __shared__ int s_stack[kWarpsPerBlock][kStackCap];
+    __shared__ int s_cand[kWarpsPerBlock][kCandCap];
+    __shared__ float4 s_batch[kWarpsPerBlock][32 * 5];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x * kWarpsPerBlock + warp;
+    if (tile >= n_tiles) return;
+    BwdTileVisitor vis;
+    vis.recs = recs;
+    vis.gperm = gperm;
+    vis.batch = s_batch[warp];
+    vis.sp = s_sorted[(int64_t)tile * 32 + lane];
+    vis.sg = s_grad[(int64_t)tile * 32 + lane];
+    vis.gacc = gacc;
+    vis.npairs = 0;
+    const float4 tlo = tile_boxes[2 * (int64_t)tile], thi = tile_boxes[2 * (int64_t)tile + 1];
+    int max_sp = 0;
+    const int st = warp_traverse(gnodes, make_float3(tlo.x, tlo.y, tlo.z), make_float3(thi.x, thi.y, thi.z),
+                                 s_stack[warp], s_cand[warp], vis, max_sp);
+    if (st && lane == 0) atomicOr(status, st);
+    if (COUNT) {
+        unsigned long long a = (unsigned long long)vis.npairs;
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+        if (lane == 0) {
+            atomicAdd(&stats[2], a);
+            atomicMax(&stats[4], (unsigned long long)max_sp);
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------
+// Finalize: gacc [P][16] (caller order) -> dmeans, dvalues, dweights and the
+// covariance adjoint dconic -> dscales, drots (one thread per Gaussian).
+// --------------------------------------------------------------------------------
+__device__ __forceinline__ void rot_cols(float r, float x, float y, float z, float Rc[3][3]) {
+    // Rc[col][row]: glm's column-major fill of forward.cu:40-44
+    Rc[0][0] = 1.f - 2.f * (y * y + z * z);
+    Rc[0][1] = 2.f * (x * y - r * z);
+    Rc[0][2] = 2.f * (x * z + r * y);
+    Rc[1][0] = 2.f * (x * y + r * z);
+    Rc[1][1] = 1.f - 2.f * (x * x + z * z);
+    Rc[1][2] = 2.f * (y * z - r * x);
+    Rc[2][0] = 2.f * (x * z - r * y);
+    Rc[2][1] = 2.f * (y * z + r * x);
+    Rc[2][2] = 1.f - 2.f * (x * x + y * y);
+}
+
+// True gradient of conic = inv(Sigma + eps I), Sigma = M^T M, M = diag(s) Rg.
+__device__ void cov_adjoint_true(const float s_in[3], const float q[4], float sm, const float c6[6],
+                                 const float u[6], float ds[3], float dq[4]) {
+    float Rc[3][3];
+    rot_cols(q[0], q[1], q[2], q[3], Rc);
+    float Rg[3][3];  // Rg[i][j] = row i, col j
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) Rg[i][j] = Rc[j][i];
+    const float sv[3] = {sm * s_in[0], sm * s_in[1], sm * s_in[2]};
+    float M[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) M[i][j] = sv[i] * Rg[i][j];
+    float Sd[3];
+    for (int i = 0; i < 3; i++) Sd[i] = M[0][i] * M[0][i] + M[1][i] * M[1][i] + M[2][i] * M[2][i];
+    const float C[3][3] = {{c6[0], c6[1], c6[2]}, {c6[1], c6[3], c6[4]}, {c6[2], c6[4], c6[5]}};
+    const float G[3][3] = {{u[0], 0.5f * u[1], 0.5f * u[2]}, {0.5f * u[1], u[3], 0.5f * u[4]}, {0.5f * u[2], 0.5f * u[4], u[5]}};
+    float T[3][3], H[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) T[i][j] = G[i][0] * C[0][j] + G[i][1] * C[1][j] + G[i][2] * C[2][j];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) H[i][j] = -(C[i][0] * T[0][j] + C[i][1] * T[1][j] + C[i][2] * T[2][j]);
+    const float a0 = fabsf(Sd[0]), a1 = fabsf(Sd[1]), a2 = fabsf(Sd[2]);
+    int kmax = 0;
+    if (a1 > a0) kmax = 1;
+    if (a2 > (kmax == 0 ? a0 : a1)) kmax = 2;
+    const float trH = H[0][0] + H[1][1] + H[2][2];
+    const float sk = Sd[kmax];
+    const float sgn = sk > 0.f ? 1.f : (sk < 0.f ? -1.f : 0.f);
+    H[kmax][kmax] += trH * 1e-5f * sgn;
+    float dM[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) dM[i][j] = 2.f * (M[i][0] * H[0][j] + M[i][1] * H[1][j] + M[i][2] * H[2][j]);
+    float GR[3][3];  // gradient wrt the textbook rotation R_std = Rg^T
+    for (int k = 0; k < 3; k++) {
+        ds[k] = (dM[k][0] * Rg[k][0] + dM[k][1] * Rg[k][1] + dM[k][2] * Rg[k][2]) * sm;
+        for (int j = 0; j < 3; j++) GR[j][k] = sv[k] * dM[k][j];
+    }
+    const float r = q[0], x = q[1], y = q[2], z = q[3];
+    dq[0] = 2.f * (-z * GR[0][1] + y * GR[0][2] + z * GR[1][0] - x * GR[1][2] - y * GR[2][0] + x * GR[2][1]);
+    dq[1] = 2.f * (y * GR[0][1] + z * GR[0][2] + y * GR[1][0] - 2.f * x * GR[1][1] - r * GR[1][2] + z * GR[2][0] +
+                   r * GR[2][1] - 2.f * x * GR[2][2]);
+    dq[2] = 2.f * (-2.f * y * GR[0][0] + x * GR[0][1] + r * GR[0][2] + x * GR[1][0] + z * GR[1][2] - r * GR[2][0] +
+                   z * GR[2][1] - 2.f * y * GR[2][2]);
+    dq[3] = 2.f * (-2.f * z * GR[0][0] - r * GR[0][1] + x * GR[0][2] + r * GR[1][0] - 2.f * z * GR[1][1] +
+                   y * GR[1][2] + x * GR[2][0] + y * GR[2][1]);
+}
+
+// Reference-compatible covariance adjoint: backward.cu:50-124 with glm's
+// column-major conventions ((A*B)[c][r] = sum_k A[k][r] * B[c][k]).
+__device__ void cov_adjoint_ref(const float s_in[3], const float q[4], float sm, const float c6[6],
+                                const float u[6], float ds[3], float dq[4]) {
+    float Rc[3][3];
+    const float r = q[0], x = q[1], y = q[2], z = q[3];
+    rot_cols(r, x, y, z, Rc);
+    const float sv[3] = {sm * s_in[0], sm * s_in[1], sm * s_in[2]};
+    auto mul = [](const float A[3][3], const float B[3][3], float O[3][3]) {
+        for (int c = 0; c < 3; c++)
+            for (int rr = 0; rr < 3; rr++) O[c][rr] = A[0][rr] * B[c][0] + A[1][rr] * B[c][1] + A[2][rr] * B[c][2];
+    };
+    float Sm[3][3] = {{sv[0], 0.f, 0.f}, {0.f, sv[1], 0.f}, {0.f, 0.f, sv[2]}};
+    float M[3][3], Mt[3][3], Sigma[3][3];
+    mul(Sm, Rc, M);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) Mt[i][j] = M[j][i];
+    mul(Mt, M, Sigma);
+    const float C[3][3] = {{c6[0], c6[1], c6[2]}, {c6[1], c6[3], c6[4]}, {c6[2], c6[4], c6[5]}};
+    const float G[3][3] = {{u[0], u[1], u[2]}, {u[1], u[3], u[4]}, {u[2], u[4], u[5]}};
+    float negC[3][3], T1[3][3], dS[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) negC[i][j] = -C[i][j];
+    mul(negC, G, T1);
+    mul(T1, C, dS);
+    const float dc[6] = {dS[0][0], dS[0][1], dS[0][2], dS[1][1], dS[1][2], dS[2][2]};
+    const float a0 = fabsf(Sigma[0][0]), a1 = fabsf(Sigma[1][1]), a2 = fabsf(Sigma[2][2]);
+    auto sgn = [](float v) { return v > 0.f ? 1.f : (v < 0.f ? -1.f : 0.f); };
+    const float de0 = (a0 >= a1 && a0 >= a2) ? 1e-5f * sgn(Sigma[0][0]) : 0.f;
+    const float de1 = (a1 >= a0 && a1 >= a2) ? 1e-5f * sgn(Sigma[1][1]) : 0.f;
+    const float de2 = (a2 >= a0 && a2 >= a1) ? 1e-5f * sgn(Sigma[2][2]) : 0.f;
+    const float tr = dc[0] + dc[3] + dc[5];
+    const float dLdS[3][3] = {{dc[0] + tr * de0, dc[1], dc[2]}, {dc[1], dc[3] + tr * de1, dc[4]}, {dc[2], dc[4], dc[5] + tr * de2}};
+    float dM[3][3], Rt[3][3], dSm[3][3];
+    mul(dLdS, M, dM);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) dM[i][j] *= 2.f;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) Rt[i][j] = Rc[j][i];
+    mul(dM, Rt, dSm);
+    ds[0] = dSm[0][0] * sm;
+    ds[1] = dSm[1][1] * sm;
+    ds[2] = dSm[2][2] * sm;
+    for (int k = 0; k < 3; k++)
+        for (int rr = 0; rr < 3; rr++) dM[k][rr] *= sv[k];
+    dq[0] = 2 * z * (dM[1][0] - dM[0][1]) + 2 * y * (dM[0][2] - dM[2][0]) + 2 * x * (dM[2][1] - dM[1][2]);
+    dq[1] = 2 * y * (dM[0][1] + dM[1][0]) + 2 * z * (dM[0][2] + dM[2][0]) + 2 * r * (dM[2][1] - dM[1][2]) -
+            4 * x * (dM[2][2] + dM[1][1]);
+    dq[2] = 2 * x * (dM[0][1] + dM[1][0]) + 2 * r * (dM[0][2] - dM[2][0]) + 2 * z * (dM[2][1] + dM[1][2]) -
+            4 * y * (dM[2][2] + dM[0][0]);
+    dq[3] = 2 * r * (dM[1][0] - dM[0][1]) + 2 * x * (dM[0][2] + dM[2][0]) + 2 * y * (dM[2][1] + dM[1][2]) -
+            4 * z * (dM[1][1] + dM[0][0]);
+}
+
+__global__ void __launch_bounds__(256) k_finalize(int P, const float* __restrict__ gacc, const float* __restrict__ scales,
+                                                  const float* __restrict__ rots, const float* __restrict__ conics,
+                                                  float sm, int ref_compat, float* __restrict__ dmeans,
+                                                  float* __restrict__ dscales, float* __restrict__ drots,
+                                                  float* __restrict__ dvalues, float* __restrict__ dweights) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const float4* a = reinterpret_cast<const float4*>(gacc + 16 * (int64_t)i);
+    const float4 a0 = a[0], a1 = a[1], a2 = a[2];
+    dvalues[i] = a0.x;
+    dweights[i] = a0.y;
+    dmeans[3 * (int64_t)i] = a0.z;
+    dmeans[3 * (int64_t)i + 1] = a0.w;
+    dmeans[3 * (int64_t)i + 2] = a1.x;
+    const float u[6] = {a1.y, a1.z, a1.w, a2.x, a2.y, a2.z};
+    const float s[3] = {scales[3 * (int64_t)i], scales[3 * (int64_t)i + 1], scales[3 * (int64_t)i + 2]};
+    const float q[4] = {rots[4 * (int64_t)i], rots[4 * (int64_t)i + 1], rots[4 * (int64_t)i + 2], rots[4 * (int64_t)i + 3]};
+    float c6[6];
+    for (int k = 0; k < 6; k++) c6[k] = conics[6 * (int64_t)i + k];
+    float ds[3], dq[4];
+    if (ref_compat) cov_adjoint_ref(s, q, sm, c6, u, ds, dq);
+    else cov_adjoint_true(s, q, sm, c6, u, ds, dq);
+    dscales[3 * (int64_t)i] = ds[0];
+    dscales[3 * (int64_t)i + 1] = ds[1];
+    dscales[3 * (int64_t)i + 2] = ds[2];
+    drots[4 * (int64_t)i] = dq[0];
+    drots[4 * (int64_t)i + 1] = dq[1];
+    drots[4 * (int64_t)i + 2] = dq[2];
+    drots[4 * (int64_t)i + 3] = dq[3];
+}
+
+// --------------------------------------------------------------------------------
+// Launchers
+// --------------------------------------------------------------------------------
+static inline unsigned nblk(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
+
+cudaError_t launch_forward(const FwdArgs& a, cudaStream_t st) {
+    if (a.n_tiles <= 0) return cudaSuccess;
+    if (a.count) {
+        k_forward<true><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
+            a.s_sorted, a.tile_boxes, (int)a.n_tiles, a.gnodes, a.recs, a.out_cells, a.out_weights, a.status, a.stats);
+    } else {
+        k_forward<false><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
+            a.s_sorted, a.tile_boxes, (int)a.n_tiles, a.gnodes, a.recs, a.out_cells, a.out_weights, a.status, a.stats);
+    }
+    gvc::note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st) {
+    if (a.P <= 0) return cudaSuccess;
+    if (a.count) {
+        k_backward_gauss<true><<<nblk(a.P, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
+            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_sorted, a.s_grad, a.tnodes,
+            a.gacc, a.status, a.stats);
+    } else {
+        k_backward_gauss<false><<<nblk(a.P, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
+            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_sorted, a.s_grad, a.tnodes,
+            a.gacc, a.status, a.stats);
+    }
+    gvc::note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_tiles(const BwdArgs& a, cudaStream_t st) {
+    if (a.n_tiles <= 0) return cudaSuccess;
+    if (a.count) {
+        k_backward_tiles<true><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
+            a.s_sorted, a.s_grad, a.tile_boxes, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc, a.status, a.stats);
+    } else {
+        k_backward_tiles<false><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
+            a.s_sorted, a.s_grad, a.tile_boxes, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc, a.status, a.stats);
+    }
+    gvc::note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(int64_t P, const float* gacc, const float* scales, const float* rots, const float* conics,
+                            float sm, int ref_compat, float* dmeans, float* dscales, float* drots, float* dvalues,
+                            float* dweights, cudaStream_t st) {
+    if (P <= 0) return cudaSuccess;
+    k_finalize<<<nblk(P, 256), 256, 0, st>>>((int)P, gacc, scales, rots, conics, sm, ref_compat, dmeans, dscales,
+                                             drots, dvalues, dweights); gvc::note_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace gvc

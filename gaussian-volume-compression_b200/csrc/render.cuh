@@ -1,0 +1,74 @@
+// render.cuh -- launch interfaces of the forward / backward evaluation kernels and
+// of the preprocessing kernels (prep.cu).
+#pragma once
+#include "gvc_internal.cuh"
+
+namespace gvc {
+
+struct FwdArgs {
+    const float4* s_sorted;
+    const float4* tile_boxes;
+    int64_t n_tiles;
+    const BvhNode* gnodes;
+    const GaussRec* recs;
+    float* out_cells;
+    float* out_weights;
+    int* status;
+    unsigned long long* stats;
+    bool count;
+};
+
+struct BwdArgs {
+    int64_t P;
+    const int32_t* gorder;  // processing order (sorted pos -> caller idx) or null
+    const int32_t* gperm;   // LBVH order -> caller idx (atomic mode)
+    const float* means;
+    const float* values;
+    const float* weights;
+    const float* conics;
+    const float4* boxes;  // caller order, lo/hi
+    const float4* s_sorted;
+    const float4* s_grad;
+    const float4* tile_boxes;
+    int64_t n_tiles;
+    const BvhNode* tnodes;  // sample-tile LBVH
+    const BvhNode* gnodes;  // Gaussian LBVH (atomic mode)
+    const GaussRec* recs;   // LBVH order (atomic mode)
+    float* gacc;            // [P][16] caller order
+    int* status;
+    unsigned long long* stats;
+    bool count;
+};
+
+cudaError_t launch_forward(const FwdArgs& a, cudaStream_t st);
+cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st);
+cudaError_t launch_backward_tiles(const BwdArgs& a, cudaStream_t st);
+cudaError_t launch_finalize(int64_t P, const float* gacc, const float* scales, const float* rots, const float* conics,
+                            float sm, int ref_compat, float* dmeans, float* dscales, float* drots, float* dvalues,
+                            float* dweights, cudaStream_t st);
+
+// prep.cu (compiled without FMA contraction so that its arithmetic matches the oracle)
+cudaError_t launch_preprocess(int64_t P, const float* means, const float* scales, const float* rots,
+                              const float* weights, float sm, float* conics_out, float4* boxes_out, cudaStream_t st);
+cudaError_t launch_gather_recs(int64_t P, const int32_t* perm, const float* means, const float* values,
+                               const float* weights, const float* conics, const float4* boxes, GaussRec* recs,
+                               cudaStream_t st);
+cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples, const int32_t* perm,
+                                const uint32_t* skeys, float4* s_sorted, float4* tile_boxes, uint32_t* tile_keys,
+                                cudaStream_t st);
+cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float* out_cells,
+                                const float* out_weights, const float* gout, const float* gw, float4* s_grad,
+                                cudaStream_t st);
+cudaError_t launch_fill_zero_outputs(int64_t S, float* out_cells, float* out_weights, cudaStream_t st);
+
+// mesh.cu
+cudaError_t launch_sample_uniform(const int64_t dims[3], const float origin[3], const float spacing[3],
+                                  const void* values, int dtype, int64_t N, const float* samples, void* out,
+                                  cudaStream_t st);
+cudaError_t launch_tet_boxes(int64_t C, const float* pts, const int32_t* conn4, float4* boxes, cudaStream_t st);
+cudaError_t launch_sample_tets(int64_t N, const float* samples, const int32_t* sperm, const float* pts,
+                               const int32_t* conn4, const double* values, const BvhNode* cnodes,
+                               const int32_t* cperm, int64_t C, double* out, int64_t* cell_ids, int* status,
+                               cudaStream_t st);
+
+}  // namespace gvc

@@ -1,0 +1,127 @@
+// traverse.cuh -- warp-cooperative LBVH traversal with a shared-memory node stack.
+//
+// One warp answers one box query (a 32-sample tile box, or one Gaussian's AABB).
+// Each round the warp pops up to 32 internal nodes (one per lane), tests both
+// children's boxes of every popped node against the query box in parallel, and
+// compacts the hits with ballots: internal children go back on the warp's stack,
+// leaves go to a candidate buffer.  Whenever 32 candidates are buffered the visitor
+// evaluates them as one batch.  The whole loop is warp-uniform (no per-thread
+// stacks, no divergence in the traversal itself), so a query issues one round of
+// independent node loads per tree level instead of one dependent load per node.
+//
+// Replaces cuBQL::fixedBoxQuery::forEachLeaf / forEachPrim as used at
+// diff-gaussian-rasterization/cuda_rasterizer/forward.cu:150,209 and
+// backward.cu:243,378 (closed-box overlap; candidates are then tested per lane).
+#pragma once
+#include "gvc_internal.cuh"
+
+namespace gvc {
+
+__device__ __forceinline__ uint32_t lane_lt_mask() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ bool box_overlap(float4 lo, float4 hi, float3 qlo, float3 qhi) {
+    return lo.x <= qhi.x && hi.x >= qlo.x && lo.y <= qhi.y && hi.y >= qlo.y && lo.z <= qhi.z && hi.z >= qlo.z;
+}
+
+// Candidate buffer capacity: a round adds at most 64 leaves to at most 31 pending.
+constexpr int kCandCap = 96;
+// Headroom kept free on the stack so that the remaining descent (one node popped
+// per round, at most one net push per level) cannot overflow.
+constexpr int kStackHeadroom = 128;
+
+// Returns 0, or kStatusStackOverflow if nodes had to be dropped (results invalid).
+// `visit(const int* cand, int nb)` is warp-collective and must end with __syncwarp().
+template <class Visitor>
+__device__ __forceinline__ int warp_traverse(const BvhNode* __restrict__ nodes, float3 qlo, float3 qhi,
+                                             int* __restrict__ stack, int* __restrict__ cand, Visitor& visit,
+                                             int& max_sp) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = lane_lt_mask();
+    int status = 0;
+    int sp = 1;
+    if (lane == 0) stack[0] = 0;
+    __syncwarp();
+    int nc = 0;
+    while (sp > 0) {
+        int k = min(sp, 32);
+        const int room = kStackCap - kStackHeadroom - sp;
+        if (k > room) k = max(room, 1);
+        const int base = sp - k;
+        const int node = (lane < k) ? stack[base + lane] : 0;
+        __syncwarp();
+        sp = base;
+        bool hl = false, hr = false;
+        uint32_t cl = 0, cr = 0;
+        if (lane < k) {
+            const float4* np = reinterpret_cast<const float4*>(nodes + node);
+            const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), d = __ldg(np + 3);
+            cl = __float_as_uint(a.w);
+            cr = __float_as_uint(b.w);
+            hl = box_overlap(a, b, qlo, qhi);
+            hr = box_overlap(c, d, qlo, qhi);
+        }
+        const bool ll = hl && (cl & kLeafBit), lr = hr && (cr & kLeafBit);
+        const bool il = hl && !(cl & kLeafBit), ir = hr && !(cr & kLeafBit);
+        const uint32_t mll = __ballot_sync(0xffffffffu, ll), mlr = __ballot_sync(0xffffffffu, lr);
+        const uint32_t mil = __ballot_sync(0xffffffffu, il), mir = __ballot_sync(0xffffffffu, ir);
+        const int nll = __popc(mll), nlr = __popc(mlr), nil = __popc(mil), nir = __popc(mir);
+        if (ll) cand[nc + __popc(mll & lt)] = (int)(cl & ~kLeafBit);
+        if (lr) cand[nc + nll + __popc(mlr & lt)] = (int)(cr & ~kLeafBit);
+        nc += nll + nlr;
+        if (sp + nil + nir > kStackCap) {
+            status = kStatusStackOverflow;
+        } else {
+            if (il) stack[sp + __popc(mil & lt)] = (int)cl;
+            if (ir) stack[sp + nil + __popc(mir & lt)] = (int)cr;
+            sp += nil + nir;
+        }
+        max_sp = max(max_sp, sp);
+        __syncwarp();
+        while (nc >= 32) {
+            visit(cand + nc - 32, 32);
+            nc -= 32;
+        }
+    }
+    if (nc > 0) visit(cand, nc);
+    return status;
+}
+
+// Sum of 16 per-lane values across the warp with 16 shuffles (recursive halving):
+// on return lanes 2k and 2k+1 hold the warp total of value k.
+__device__ __forceinline__ float warp_transpose_reduce16(float (&v)[16]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const bool up = lane & 16;
+        float send = up ? v[i] : v[i + 8];
+        float keep = up ? v[i + 8] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const bool up = lane & 8;
+        float send = up ? v[i] : v[i + 4];
+        float keep = up ? v[i + 4] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const bool up = lane & 4;
+        float send = up ? v[i] : v[i + 2];
+        float keep = up ? v[i + 2] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+    {
+        const bool up = lane & 2;
+        float send = up ? v[0] : v[1];
+        float keep = up ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+}  // namespace gvc

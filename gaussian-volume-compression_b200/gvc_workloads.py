@@ -1,0 +1,97 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+The reference measures on no public dataset (its trained meshes are not shipped), so
+every configuration is a seeded synthetic stand-in with the shapes, sizes and value
+distributions the configuration names.  Used by bench.py and by the tests.
+"""
+import numpy as np
+
+
+def mixture_small(seed=0, P=4096):
+    """Config 1: P anisotropic Gaussians, mu ~ U[0,1]^3, log-scales ~ N(log 0.02, 0.3),
+    random unit quaternions, w = sigmoid(N(0,1)), v ~ U[0,1] (activated, float32)."""
+    rng = np.random.default_rng(seed)
+    means = rng.random((P, 3), dtype=np.float32)
+    scales = np.exp(rng.normal(np.log(0.02), 0.3, (P, 3))).astype(np.float32)
+    q = rng.normal(size=(P, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    weights = (1.0 / (1.0 + np.exp(-rng.normal(size=P)))).astype(np.float32)
+    values = rng.random(P, dtype=np.float32)
+    return means, scales, q.astype(np.float32), values, weights
+
+
+def grid_centres(n=64):
+    """The n^3 cell centres (i + 0.5) / n of [0,1]^3 (x fastest)."""
+    c = (np.arange(n, dtype=np.float32) + 0.5) / n
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1).astype(np.float32)
+
+
+def blob_target(samples, seed=0, nblobs=16):
+    """Config 1 target: sum of isotropic blobs (centres U[0,1]^3, sigma U[0.05,0.15],
+    amplitude U[0.5,1])."""
+    rng = np.random.default_rng(seed + 1000)
+    c = rng.random((nblobs, 3))
+    sg = rng.uniform(0.05, 0.15, nblobs)
+    a = rng.uniform(0.5, 1.0, nblobs)
+    d2 = ((samples[:, None, :].astype(np.float64) - c[None]) ** 2).sum(-1)
+    return (a[None] * np.exp(-0.5 * d2 / sg[None] ** 2)).sum(-1)
+
+
+def mixture_large(seed=0, P=2_000_000, S=16_000_000):
+    """Config 4: P Gaussians clustered around 256 centres (sigma 0.05, clamped to
+    [0,1]), log-scales ~ N(log 0.004, 0.4), random quaternions, v ~ U[0,1],
+    w = sigmoid(N(0,1)); S/2 uniform samples + S/2 samples at mu_j + N(0, s_j^2)."""
+    rng = np.random.default_rng(seed)
+    centres = rng.random((256, 3))
+    lab = rng.integers(0, 256, P)
+    means = np.clip(centres[lab] + rng.normal(0, 0.05, (P, 3)), 0, 1).astype(np.float32)
+    scales = np.exp(rng.normal(np.log(0.004), 0.4, (P, 3))).astype(np.float32)
+    q = rng.normal(size=(P, 4)).astype(np.float32)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    values = rng.random(P, dtype=np.float32)
+    weights = (1.0 / (1.0 + np.exp(-rng.normal(size=P)))).astype(np.float32)
+    half = S // 2
+    uni = rng.random((half, 3), dtype=np.float32)
+    j = rng.integers(0, P, S - half)
+    near = (means[j] + rng.normal(size=(S - half, 3)).astype(np.float32) * scales[j]).astype(np.float32)
+    samples = np.concatenate([uni, near], axis=0)
+    return means, scales, q, values, weights, samples
+
+
+def jittered_tet_mesh(n=16, seed=0, jitter=0.2):
+    """Config 3 geometry: an n^3 hex grid on [0,1]^3, interior vertices jittered by
+    U[-jitter, jitter]*h, each hex split into 6 tets along its main diagonal (Kuhn
+    split: vertex 0 -> 7 of every tet, declared).  Returns (pts [V,3] f32, tets [C,4])."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 / n
+    c = np.arange(n + 1) * h
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    pts = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    interior = np.all((pts > 0.5 * h) & (pts < 1 - 0.5 * h), axis=1)
+    pts[interior] += rng.uniform(-jitter, jitter, (interior.sum(), 3)) * h
+    pts = pts.astype(np.float32)
+    N1 = n + 1
+    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+
+    def vid(di, dj, dk):
+        return (k + dk) * N1 * N1 + (j + dj) * N1 + (i + di)
+
+    v = [vid(0, 0, 0), vid(1, 0, 0), vid(0, 1, 0), vid(1, 1, 0), vid(0, 0, 1), vid(1, 0, 1), vid(0, 1, 1), vid(1, 1, 1)]
+    # the six monotone lattice paths from corner 0 to corner 7 (x=1, y=2, z=4 bit steps)
+    paths = [(1, 2, 4), (1, 4, 2), (2, 1, 4), (2, 4, 1), (4, 1, 2), (4, 2, 1)]
+    tets = []
+    for a, b, _ in paths:
+        tets.append(np.stack([v[0], v[a], v[a | b], v[7]], axis=1))
+    tets = np.stack(tets, axis=1).reshape(-1, 4).astype(np.int64)
+    return pts, tets
+
+
+def blob_field(pts, seed=0, nblobs=32):
+    rng = np.random.default_rng(seed + 7)
+    c = rng.random((nblobs, 3))
+    sg = rng.uniform(0.05, 0.2, nblobs)
+    a = rng.uniform(0.2, 1.0, nblobs)
+    d2 = ((pts[:, None, :].astype(np.float64) - c[None]) ** 2).sum(-1)
+    return (a[None] * np.exp(-0.5 * d2 / sg[None] ** 2)).sum(-1).astype(np.float32)

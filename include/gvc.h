@@ -1,0 +1,150 @@
+/*
+ * gvc.h -- C ABI of the B200 Gaussian-mixture volume path (libgvc.so).
+ *
+ * Plain pointers and sizes only: every float / int pointer below is a DEVICE pointer
+ * on the context's device unless stated otherwise, and `stream` is a cudaStream_t
+ * passed as void* (NULL = legacy default stream).  All calls are stream-ordered and
+ * do not synchronise the device unless `debug` is non-zero.
+ *
+ * Each entry point names the reference interface it replaces (paths inside the
+ * reference project schakrabarti-lanl/gaussian-volume-compression).
+ *
+ * Return value: 0 (GVC_OK) or a gvc_status code; gvc_last_error() gives the message.
+ * Device-side failures (a traversal stack overflow) are recorded in a status word and
+ * reported by gvc_sync_status() and by the next call on the same context.
+ */
+#ifndef GVC_H_INCLUDED
+#define GVC_H_INCLUDED
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gvc_ctx gvc_ctx;
+
+typedef enum {
+    GVC_OK = 0,
+    GVC_ERR_ARG = 1,         /* bad argument (shape, size, null pointer, dtype)      */
+    GVC_ERR_CUDA = 2,        /* a CUDA runtime call failed                            */
+    GVC_ERR_CAPACITY = 3,    /* a size exceeds a documented maximum                   */
+    GVC_ERR_TRAVERSAL = 4,   /* a BVH traversal stack overflowed (results invalid)    */
+    GVC_ERR_UNSUPPORTED = 5, /* unsupported cell type / dtype                         */
+    GVC_ERR_STATE = 6        /* call order violated (forward before build_bvh, ...)   */
+} gvc_status;
+
+/* Options for gvc_set_option. */
+typedef enum {
+    GVC_OPT_COV_GRAD = 1,   /* 0 = true gradient of the forward (default),
+                               1 = reference-compatible formula of
+                                   diff-gaussian-rasterization/cuda_rasterizer/backward.cu:50-124 */
+    GVC_OPT_BWD_MODE = 2,   /* 0 = follow use_gaussian_bvh (default):
+                                   use_gaussian_bvh == 0 -> Gaussian-owned segmented reduction
+                                   (deterministic, no atomics; mirrors backward.cu:127-337),
+                                   use_gaussian_bvh != 0 -> sample-tile traversal with warp
+                                   pre-reduction + FP32 atomics (mirrors backward.cu:339-559);
+                               1 = always deterministic, 2 = always atomic                */
+    GVC_OPT_EVAL_PATH = 3,  /* 0 = plain FP32 CUDA-core exponent (default),
+                               1 = tensor-core (tcgen05) BF16 split exponent                */
+    GVC_OPT_COUNT_PAIRS = 4,/* 1 = record per-call pair counts (gvc_get_stats)            */
+    GVC_OPT_TIME_KERNELS = 5 /* 1 = time the evaluation kernels with CUDA events on the
+                                caller's stream (gvc_get_stats)                          */
+} gvc_option;
+
+typedef struct {
+    int64_t fwd_candidates;   /* (sample, Gaussian) pairs with the sample inside the AABB   */
+    int64_t fwd_contributing; /* ... and -14 <= power <= 0                                  */
+    int64_t bwd_contributing; /* contributing pairs of samples with W > 0.01                */
+    int32_t max_stack_fwd;    /* deepest traversal stack seen (entries)                     */
+    int32_t max_stack_bwd;
+    double fwd_kernel_ms;     /* summed duration of the forward evaluation kernel          */
+    double bwd_kernel_ms;     /* summed duration of the backward evaluation kernel         */
+    int64_t fwd_kernel_calls; /* launches timed since the option was set                   */
+    int64_t bwd_kernel_calls;
+} gvc_stats;
+
+/* Context: owns the sample ordering, both LBVHs and all workspace (no per-call
+   cudaMalloc once sizes stop growing).  Replaces the module statics samples_bvh,
+   gaussian_bvh and stored_samples of diff-gaussian-rasterization/ext.cu:8-10.
+   A context belongs to the device current at creation; use one context per thread. */
+int gvc_ctx_create(gvc_ctx** out);
+void gvc_ctx_destroy(gvc_ctx* ctx);
+const char* gvc_last_error(const gvc_ctx* ctx);
+int gvc_set_option(gvc_ctx* ctx, int option, int value);
+int gvc_get_stats(gvc_ctx* ctx, gvc_stats* out, void* stream); /* synchronises `stream` */
+/* Number of kernel launches this library has issued in the process so far (all
+   contexts); no counterpart in the reference. */
+int64_t gvc_launch_count(void);
+/* Waits for `stream`, returns the device status word (GVC_OK or GVC_ERR_TRAVERSAL) and clears it. */
+int gvc_sync_status(gvc_ctx* ctx, void* stream);
+
+/* Replaces BuildBVH (diff-gaussian-rasterization/ext.cu:28-65).
+   samples: [S,3] float32.  The context keeps the POINTER: the caller keeps the buffer
+   alive and unchanged until the next gvc_build_bvh (the reference keeps a tensor
+   reference, ext.cu:29).  Sorts the samples by a 30-bit Morton key, forms 32-sample
+   tiles and builds the tile LBVH (the reference's leaf threshold 257, ext.cu:51, has
+   no counterpart: tiles are 32 samples). */
+int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int use_gaussian_bvh, void* stream);
+
+/* Replaces RasterizeGaussiansCUDAWrapper / RasterizeGaussiansCUDA
+   (diff-gaussian-rasterization/ext.cu:67-105, rasterize_points.cu:17-73).
+   means3D [P,3], scales [P,3], rotations [P,4] (r,x,y,z), values [P], weights [P];
+   bounds = {min_x, min_y, min_z, max_x, max_y, max_z} and bg are accepted and unused,
+   as in the reference.  Outputs (caller-allocated): out_cells [S], out_weights [S],
+   conics [6P].  P == 0 writes zeros (rasterize_points.cu:51). */
+int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const float* scales,
+                            const float* rotations, const float* values, const float* weights, float scale_modifier,
+                            const float* bounds /* host, 6 floats, may be NULL */, float bg, int use_gaussian_bvh,
+                            int debug, float* out_cells, float* out_weights, float* conics, void* stream);
+
+/* Replaces RasterizeGaussiansBackwardCUDAWrapper / RasterizeGaussiansBackwardCUDA
+   (diff-gaussian-rasterization/ext.cu:107-147, rasterize_points.cu:75-137).
+   Outputs (caller-allocated, overwritten): dmeans [P,3], dscales [P,3], drots [P,4],
+   dvalues [P], dweights [P]. */
+int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means3D, const float* scales,
+                                     const float* rotations, const float* conics, const float* values,
+                                     const float* weights, const float* out_cells, const float* out_weights,
+                                     float scale_modifier, const float* bounds, float bg, const float* dL_dout_cells,
+                                     const float* dL_dout_weights, int use_gaussian_bvh, int debug, float* dmeans,
+                                     float* dscales, float* drots, float* dvalues, float* dweights, void* stream);
+
+/* Value dtypes of the structured sampler (gpu_sampling/sample_mesh.cu:76-115). */
+typedef enum { GVC_F64 = 0, GVC_F32 = 1, GVC_U16 = 2, GVC_U8 = 3 } gvc_dtype;
+
+/* Replaces sample_mesh (gpu_sampling/sample_mesh.cu:26-240): uniform point field of
+   dims nx*ny*nz (x fastest), trilinear interpolation, invalid = -1 cast to the dtype.
+   dims/origin/spacing are HOST arrays; values/samples/out are device pointers. */
+int gvc_sample_uniform(gvc_ctx* ctx, const int64_t* dims, const float* origin, const float* spacing,
+                       const void* values, int dtype, int64_t N, const float* samples, void* out, void* stream);
+
+/* Replaces the tetrahedral case of sample_meshu (gpu_sampling/sample_mesh.cu:242-414,
+   VTK_TETRA = 10).  conn4: [C,4] int32 vertex ids; values: [npts] float64.
+   out: [N] float64 (value or -1); cell_ids: [N] int64 (lowest containing tet or -1),
+   may be NULL. */
+int gvc_sample_tets(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, const int32_t* conn4,
+                    const double* values, int64_t N, const float* samples, double* out, int64_t* cell_ids,
+                    void* stream);
+
+/* Test hook: builds the LBVH over n boxes [n,6] (lo xyz, hi xyz) exactly as the
+   forward does over Gaussian AABBs, and copies the result out (device pointers):
+   keys_sorted [n] uint32, perm [n] int32, left/right [n-1] int32 (leaf i encoded as
+   i | 0x80000000), node_boxes [(n-1),6]. No counterpart in the reference (its
+   builder is cuBQL::cuda::radixBuilder, rasterizer_impl.cu:82). */
+int gvc_debug_lbvh(gvc_ctx* ctx, int64_t n, const float* boxes, uint32_t* keys_sorted, int32_t* perm,
+                   int32_t* left, int32_t* right, float* node_boxes, void* stream);
+
+/* Test hook: the forward's preprocess (FORWARD::preprocess, forward.cu:10-114) alone:
+   conics [6P] and AABBs [P,6] in the caller's order. */
+int gvc_debug_preprocess(gvc_ctx* ctx, int64_t P, const float* means3D, const float* scales, const float* rotations,
+                         const float* weights, float scale_modifier, float* conics, float* aabbs, void* stream);
+
+/* Test hook: the sample ordering of the last gvc_build_bvh: perm [S] int32 (sorted
+   position -> caller index) and keys [S] uint32. */
+int gvc_debug_sample_order(gvc_ctx* ctx, int32_t* perm, uint32_t* keys, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GVC_H_INCLUDED */

@@ -1,0 +1,60 @@
+"""CPU checks of the mesh-sampling oracle: exactness on linear / trilinear fields, no
+gaps between tets, the lowest-id tie-break, the invalid value."""
+import numpy as np
+
+
+def test_uniform_reproduces_trilinear_field(orc):
+    rng = np.random.default_rng(0)
+    dims = np.array([7, 5, 9])
+    origin = np.array([-0.5, 0.25, 0.0], np.float32)
+    spacing = np.array([0.25, 0.5, 0.125], np.float32)
+    i, j, k = np.meshgrid(np.arange(7), np.arange(5), np.arange(9), indexing="ij")
+    X = origin[0] + i * spacing[0]
+    Y = origin[1] + j * spacing[1]
+    Z = origin[2] + k * spacing[2]
+    f = lambda x, y, z: 1.0 + 2 * x - 3 * y + 0.5 * z + 0.25 * x * y * z
+    vals = np.transpose(f(X, Y, Z), (2, 1, 0)).reshape(-1)  # x fastest
+    hi = origin + (dims - 1) * spacing
+    pts = (origin + rng.random((2000, 3)) * (hi - origin)).astype(np.float32)
+    pts = np.concatenate([pts, [hi.astype(np.float32), origin, hi + 0.01, origin - 0.01]]).astype(np.float32)
+    out, valid = orc.sample_uniform(dims, origin, spacing, vals, pts)
+    p = pts.astype(np.float64)
+    assert valid[:-2].all() and not valid[-2:].any()
+    np.testing.assert_allclose(out[:-2], f(p[:-2, 0], p[:-2, 1], p[:-2, 2]), rtol=1e-12, atol=1e-12)
+
+
+def test_tets_interpolate_linear_field_without_gaps(orc):
+    pts, tets = orc.jittered_tet_mesh(n=6, seed=1)
+    a = np.array([0.3, -1.2, 2.0])
+    vals = pts.astype(np.float64) @ a + 0.7
+    rng = np.random.default_rng(2)
+    q = rng.random((5000, 3)).astype(np.float32)
+    out, cell = orc.sample_tets(pts, tets, vals, q)
+    assert (cell >= 0).all()
+    np.testing.assert_allclose(out, q.astype(np.float64) @ a + 0.7, rtol=0, atol=1e-9)
+    out2, cell2 = orc.sample_tets(pts, tets, vals, np.array([[1.5, 0.5, 0.5], [-0.1, 0.2, 0.3]], np.float32))
+    assert (cell2 == -1).all() and (out2 == -1.0).all()
+
+
+def test_tets_lowest_id_on_shared_vertex(orc):
+    pts, tets = orc.jittered_tet_mesh(n=3, seed=0, jitter=0.0)
+    # a grid vertex is shared by many tets: the lowest containing id wins
+    v = np.array([[1 / 3, 1 / 3, 1 / 3]], np.float32)
+    out, cell = orc.sample_tets(pts, tets, np.arange(pts.shape[0], dtype=np.float64), v)
+    owners = [c for c in range(tets.shape[0]) if (np.abs(pts[tets[c]] - v).sum(1) < 1e-7).any()]
+    assert cell[0] == min(owners)
+
+
+def test_tet_grid_search_matches_brute_force(orc):
+    pts, tets = orc.jittered_tet_mesh(n=4, seed=3)
+    rng = np.random.default_rng(4)
+    q = rng.random((300, 3)).astype(np.float32)
+    out, cell = orc.sample_tets(pts, tets, np.zeros(pts.shape[0]), q)
+    for s in range(q.shape[0]):
+        best = -1
+        for c in range(tets.shape[0]):
+            _, cc = orc.sample_tets(pts, tets[c:c + 1], np.zeros(pts.shape[0]), q[s:s + 1])
+            if cc[0] == 0:
+                best = c
+                break
+        assert best == cell[s]
