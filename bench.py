@@ -291,7 +291,11 @@ def run_ours(args):
                 "fp32_simt_nominal_tflops": FP32_NOMINAL_TFLOPS,
                 "frac_of_fp32_simt_nominal": achieved / FP32_NOMINAL_TFLOPS,
                 "fwd_kernel_ms": t_fwd, "bwd_kernel_ms": t_bwd,
-                "pairs": {"candidates": n_cand, "fwd_contributing": n_fc, "bwd_contributing": n_bc},
+                "pairs": {"candidates": n_cand, "fwd_contributing": n_fc, "bwd_contributing": n_bc,
+                          "fwd_tile_gaussian_evals": counts["fwd_leaf_hits"],
+                          "fwd_node_visits": counts["fwd_node_visits"],
+                          "bwd_leaf_evals": counts["bwd_leaf_hits"],
+                          "bwd_node_visits": counts["bwd_node_visits"]},
                 "flops_per_pair": {"candidate": F_CAND, "fwd_contributing": F_FWD_CONTRIB,
                                    "bwd_contributing": F_BWD_CONTRIB, "ex2_fp32_equiv": EX2_EQUIV}}
 

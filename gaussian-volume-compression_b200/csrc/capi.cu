@@ -166,8 +166,8 @@ int gvc_ctx_create(gvc_ctx** out) {
     GVC_CUDA(cudaGetDevice(&c->device), "cudaGetDevice");
     GVC_CUDA(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc status");
     GVC_CUDA(cudaMemset(c->d_status, 0, sizeof(int)), "cudaMemset status");
-    GVC_CUDA(cudaMalloc(&c->d_stats, sizeof(unsigned long long) * 8), "cudaMalloc stats");
-    GVC_CUDA(cudaMemset(c->d_stats, 0, sizeof(unsigned long long) * 8), "cudaMemset stats");
+    GVC_CUDA(cudaMalloc(&c->d_stats, sizeof(unsigned long long) * 16), "cudaMalloc stats");
+    GVC_CUDA(cudaMemset(c->d_stats, 0, sizeof(unsigned long long) * 16), "cudaMemset stats");
     GVC_CUDA(cudaMallocHost(&c->h_status, sizeof(int)), "cudaMallocHost");
     *out = c;
     return GVC_OK;
@@ -185,7 +185,7 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
                           &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds};
         for (DevBuf* b : bufs) b->release();
     }
-    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->s_grad, &c->grec, &c->gtmp,
+    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->s_grad, &c->grec, &c->gtmp,
                       &c->m_out_sorted, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
     for (DevBuf* b : bufs) b->release();
     if (c->d_status) cudaFree(c->d_status);
@@ -231,7 +231,7 @@ int gvc_set_option(gvc_ctx* ctx, int option, int value) {
 int gvc_get_stats(gvc_ctx* ctx, gvc_stats* out, void* stream) {
     if (!ctx || !out) return GVC_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    unsigned long long h[8];
+    unsigned long long h[16];
     GVC_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     GVC_CUDA(cudaMemcpy(h, ctx->d_stats, sizeof(h), cudaMemcpyDeviceToHost), "stats copy");
     out->fwd_candidates = (int64_t)h[0];
@@ -239,6 +239,10 @@ int gvc_get_stats(gvc_ctx* ctx, gvc_stats* out, void* stream) {
     out->bwd_contributing = (int64_t)h[2];
     out->max_stack_fwd = (int32_t)h[3];
     out->max_stack_bwd = (int32_t)h[4];
+    out->fwd_leaf_hits = (int64_t)h[5];
+    out->fwd_node_visits = (int64_t)h[6];
+    out->bwd_leaf_hits = (int64_t)h[7];
+    out->bwd_node_visits = (int64_t)h[8];
     drain_events(ctx);
     out->fwd_kernel_ms = ctx->fwd_kernel_ms;
     out->bwd_kernel_ms = ctx->bwd_kernel_ms;
@@ -268,15 +272,17 @@ int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int 
         GVC_CUDA(morton_sort_points(ctx->s_sort, S, samples, st), "sample sort");
         const int64_t slots = ctx->n_tiles * kTile;
         GVC_CUDA(ctx->s_sorted.ensure(sizeof(float4) * slots), "alloc s_sorted");
-        GVC_CUDA(ctx->tile_boxes.ensure(sizeof(float4) * 2 * ctx->n_tiles), "alloc tile_boxes");
-        GVC_CUDA(ctx->tile_keys.ensure(sizeof(uint32_t) * ctx->n_tiles), "alloc tile_keys");
+        const int64_t slots_g = ctx->n_tiles * kGroups;
+        GVC_CUDA(ctx->tile_boxes.ensure(sizeof(float4) * 2 * slots_g), "alloc tile_boxes");
+        GVC_CUDA(ctx->tile_keys.ensure(sizeof(uint32_t) * slots_g), "alloc tile_keys");
+        GVC_CUDA(ctx->tile_gdesc.ensure(sizeof(uint32_t) * ctx->n_tiles), "alloc tile_gdesc");
         GVC_CUDA(launch_sample_tiles(S, ctx->n_tiles, samples, ctx->s_sort.perm.as<int32_t>(),
                                      ctx->s_sort.keys.as<uint32_t>(), ctx->s_sorted.as<float4>(),
-                                     ctx->tile_boxes.as<float4>(), ctx->tile_keys.as<uint32_t>(), st),
+                                     ctx->tile_boxes.as<float4>(), ctx->tile_keys.as<uint32_t>(),
+                                     ctx->tile_gdesc.as<uint32_t>(), st),
                  "sample tiles");
-        GVC_CUDA(lbvh_hierarchy(ctx->tiles, ctx->n_tiles, ctx->tile_keys.as<uint32_t>(),
-                                ctx->tile_boxes.as<float4>(), st),
-                 "tile LBVH");
+        GVC_CUDA(lbvh_hierarchy(ctx->tiles, slots_g, ctx->tile_keys.as<uint32_t>(), ctx->tile_boxes.as<float4>(), st),
+                 "sample-group LBVH");
     }
     ctx->samples_ready = true;
     tm.mark();
@@ -309,7 +315,7 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
     if (!means3D || !scales || !rotations || !values || !weights || !conics)
         return fail(ctx, GVC_ERR_ARG, "null Gaussian parameter pointer");
     DebugTimer tm(debug != 0, st);
-    if (ctx->count_pairs) GVC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, sizeof(unsigned long long) * 8, st), "stats");
+    if (ctx->count_pairs) GVC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, sizeof(unsigned long long) * 16, st), "stats");
     tm.mark();
     GVC_CUDA(ctx->gtmp.ensure(sizeof(float4) * 2 * P), "alloc boxes");
     float4* boxes = ctx->gtmp.as<float4>();
@@ -325,6 +331,7 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
     FwdArgs fa;
     fa.s_sorted = ctx->s_sorted.as<float4>();
     fa.tile_boxes = ctx->tile_boxes.as<float4>();
+    fa.gdesc = ctx->tile_gdesc.as<uint32_t>();
     fa.n_tiles = ctx->n_tiles;
     fa.gnodes = ctx->gbvh.nodes.as<BvhNode>();
     fa.recs = ctx->grec.as<GaussRec>();
@@ -397,6 +404,7 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
         ba.s_sorted = ctx->s_sorted.as<float4>();
         ba.s_grad = ctx->s_grad.as<float4>();
         ba.tile_boxes = ctx->tile_boxes.as<float4>();
+        ba.gdesc = ctx->tile_gdesc.as<uint32_t>();
         ba.n_tiles = ctx->n_tiles;
         ba.tnodes = ctx->tiles.nodes.as<BvhNode>();
         ba.gacc = gacc;

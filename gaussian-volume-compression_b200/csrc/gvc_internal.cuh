@@ -14,8 +14,11 @@ constexpr float kWeightCutoff = 1e-2f;
 constexpr float kPowerFloor = -14.0f;
 // Tile of Morton-sorted samples handled by one warp.
 constexpr int kTile = 32;
+// Each tile is split into at most this many lane groups at Morton-order jumps; the
+// sample-side LBVH has one leaf slot per (tile, group).
+constexpr int kGroups = 4;
 // Per-warp traversal stack (entries of int32) in shared memory.
-constexpr int kStackCap = 1024;
+constexpr int kStackCap = 512;
 // Gaussians whose covariance condition estimate exceeds this get an FP64 inverse.
 constexpr float kCondFp64 = 1.0e2f;
 
@@ -106,8 +109,10 @@ struct gvc_ctx {
     int64_t n_tiles = 0;
     bool samples_ready = false;
     gvc::DevBuf s_sorted;   // [n_tiles*32] float4 (x, y, z, bits of caller index or -1)
-    gvc::DevBuf tile_boxes; // [n_tiles] 2 x float4
-    gvc::DevBuf tile_keys;  // [n_tiles] uint32
+    gvc::DevBuf tile_boxes; // [n_tiles * kGroups] group boxes, 2 x float4 (empty for unused slots)
+    gvc::DevBuf tile_keys;  // [n_tiles * kGroups] uint32 Morton key of each group's first sample
+    gvc::DevBuf tile_gdesc; // [n_tiles] group starts: bytes 0..2 = start lane of groups 1..3
+                            // (32 if unused), byte 3 = number of groups
     gvc::DevBuf s_grad;     // [n_tiles*32] float4 (out, outw, dL_dout, dL_doutw) for the backward
     gvc::Lbvh s_sort;       // sample sort (keys/perm only)
     gvc::Lbvh tiles;        // tile LBVH
@@ -122,6 +127,6 @@ struct gvc_ctx {
     gvc::DevBuf m_out_sorted;
     // status and statistics
     int* d_status = nullptr;          // device status word
-    unsigned long long* d_stats = nullptr;  // [8] device counters
+    unsigned long long* d_stats = nullptr;  // [16] device counters
     int* h_status = nullptr;          // pinned mirror
 };

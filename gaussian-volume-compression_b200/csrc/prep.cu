@@ -99,7 +99,8 @@ __device__ void aabb_of(const float mu[3], const float s_in[3], const float q[4]
     float Rc[3][3];
     rot_cols_p(q[0], q[1], q[2], q[3], Rc);
     const float S0 = sm * s_in[0], S1 = sm * s_in[1], S2 = sm * s_in[2];
-    const float arg = (float)((0.1 * (double)kWeightCutoff) / (double)w);
+    // (0.1 * WEIGHT_CUTOFF) with the reference's double literal 1e-2 (config.h:9)
+    const float arg = (float)((0.1 * 1e-2) / (double)w);
     const float m = (float)sqrt(-2.0 * log((double)arg));
     const float ss0 = S0 * m, ss1 = S1 * m, ss2 = S2 * m;
     const float n[2] = {-1.0f, 1.0f};
@@ -165,42 +166,110 @@ __global__ void __launch_bounds__(256) k_gather_recs(int64_t P, const int32_t* _
 }
 
 // Sorted sample slots: (x, y, z, caller index as int bits); padding slots carry NaN
-// coordinates and index -1.  One warp per tile also reduces the tile box.
+// coordinates and index -1.  One warp per tile of 32 slots also splits the tile into at
+// most kGroups contiguous lane groups: a group [a, b) is split at the Morton bit where
+// its first and last keys first differ when both halves' boxes are at most half the
+// group's size (half-perimeter).  A tile that straddles a jump of the Z-order curve thus
+// becomes compact groups instead of one box spanning the jump.  Writes one box and
+// key per group slot (unused slots: empty box, key of the last sample) and the group
+// descriptor of the tile.
+struct WBox {
+    float lx, ly, lz, hx, hy, hz;
+};
+
+__device__ __forceinline__ WBox warp_box(bool in, float x, float y, float z) {
+    WBox b;
+    b.lx = in ? x : INFINITY;
+    b.ly = in ? y : INFINITY;
+    b.lz = in ? z : INFINITY;
+    b.hx = in ? x : -INFINITY;
+    b.hy = in ? y : -INFINITY;
+    b.hz = in ? z : -INFINITY;
+    for (int off = 16; off > 0; off >>= 1) {
+        b.lx = fminf(b.lx, __shfl_xor_sync(0xffffffffu, b.lx, off));
+        b.ly = fminf(b.ly, __shfl_xor_sync(0xffffffffu, b.ly, off));
+        b.lz = fminf(b.lz, __shfl_xor_sync(0xffffffffu, b.lz, off));
+        b.hx = fmaxf(b.hx, __shfl_xor_sync(0xffffffffu, b.hx, off));
+        b.hy = fmaxf(b.hy, __shfl_xor_sync(0xffffffffu, b.hy, off));
+        b.hz = fmaxf(b.hz, __shfl_xor_sync(0xffffffffu, b.hz, off));
+    }
+    return b;
+}
+
+__device__ __forceinline__ float half_perimeter(const WBox& b) {
+    return (b.hx - b.lx) + (b.hy - b.ly) + (b.hz - b.lz);
+}
+
+// Split lane of group [a, b), or -1 (warp-uniform).
+__device__ int try_split(int a, int b, uint32_t key, int lane, float x, float y, float z) {
+    if (b - a < 2) return -1;
+    const uint32_t ka = __shfl_sync(0xffffffffu, key, a), kb = __shfl_sync(0xffffffffu, key, b - 1);
+    if (ka == kb) return -1;
+    const int bit = 31 - __clz(ka ^ kb);
+    const bool in = lane >= a && lane < b;
+    const uint32_t hi = __ballot_sync(0xffffffffu, in && ((key >> bit) & 1u));
+    const int m = __ffs(hi) - 1;  // keys are sorted: a < m < b
+    const WBox B = warp_box(in, x, y, z);
+    const WBox B1 = warp_box(in && lane < m, x, y, z);
+    const WBox B2 = warp_box(in && lane >= m, x, y, z);
+    const float h = half_perimeter(B);
+    return fmaxf(half_perimeter(B1), half_perimeter(B2)) <= 0.5f * h ? m : -1;
+}
+
 __global__ void __launch_bounds__(256) k_sample_tiles(int64_t S, int64_t n_tiles, const float* __restrict__ samples,
                                                       const int32_t* __restrict__ perm,
                                                       const uint32_t* __restrict__ skeys, float4* __restrict__ s_sorted,
-                                                      float4* __restrict__ tile_boxes, uint32_t* __restrict__ tile_keys) {
+                                                      float4* __restrict__ group_boxes, uint32_t* __restrict__ group_keys,
+                                                      uint32_t* __restrict__ gdesc) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t t = i >> 5;
     if (t >= n_tiles) return;
     const int lane = threadIdx.x & 31;
     float x = NAN, y = NAN, z = NAN;
     int o = -1;
+    uint32_t key = 0xffffffffu;
     if (i < S) {
         o = perm[i];
         x = samples[3 * (int64_t)o];
         y = samples[3 * (int64_t)o + 1];
         z = samples[3 * (int64_t)o + 2];
+        key = skeys[i];
     }
     s_sorted[i] = make_float4(x, y, z, __int_as_float(o));
-    float lx = x, ly = y, lz = z, hx = x, hy = y, hz = z;
-    if (o < 0) {
-        lx = ly = lz = INFINITY;
-        hx = hy = hz = -INFINITY;
+    const int nvalid = __popc(__ballot_sync(0xffffffffu, o >= 0));
+    int starts[kGroups + 1];
+    int ng = 1;
+    starts[0] = 0;
+    const int m = try_split(0, nvalid, key, lane, x, y, z);
+    if (m >= 0) {
+        const int m1 = try_split(0, m, key, lane, x, y, z);
+        const int m2 = try_split(m, nvalid, key, lane, x, y, z);
+        if (m1 >= 0) starts[ng++] = m1;
+        starts[ng++] = m;
+        if (m2 >= 0) starts[ng++] = m2;
     }
-    for (int off = 16; off > 0; off >>= 1) {
-        lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, off));
-        ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, off));
-        lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, off));
-        hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, off));
-        hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, off));
-        hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, off));
+    for (int g = ng; g <= kGroups; g++) starts[g] = 32;
+    const uint32_t last_key = __shfl_sync(0xffffffffu, key, nvalid - 1);
+    for (int g = 0; g < kGroups; g++) {
+        const int a = starts[g], b = (g + 1 < ng) ? starts[g + 1] : nvalid;
+        WBox B;
+        uint32_t k = last_key;
+        if (g < ng) {
+            B = warp_box(lane >= a && lane < b, x, y, z);
+            k = __shfl_sync(0xffffffffu, key, a);
+        } else {
+            B.lx = B.ly = B.lz = INFINITY;
+            B.hx = B.hy = B.hz = -INFINITY;
+        }
+        if (lane == 0) {
+            group_boxes[2 * (kGroups * t + g)] = make_float4(B.lx, B.ly, B.lz, 0.f);
+            group_boxes[2 * (kGroups * t + g) + 1] = make_float4(B.hx, B.hy, B.hz, 0.f);
+            group_keys[kGroups * t + g] = k;
+        }
     }
-    if (lane == 0) {
-        tile_boxes[2 * t] = make_float4(lx, ly, lz, 0.f);
-        tile_boxes[2 * t + 1] = make_float4(hx, hy, hz, 0.f);
-        tile_keys[t] = skeys[t * 32];
-    }
+    if (lane == 0)
+        gdesc[t] = (uint32_t)starts[1] | ((uint32_t)starts[2] << 8) | ((uint32_t)starts[3] << 16) |
+                   ((uint32_t)ng << 24);
 }
 
 // Per sorted sample: (gO / W, -gO * out / W, gW, 1) if W > 0.01, else zeros
@@ -242,11 +311,11 @@ cudaError_t launch_gather_recs(int64_t P, const int32_t* perm, const float* mean
 }
 
 cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples, const int32_t* perm,
-                                const uint32_t* skeys, float4* s_sorted, float4* tile_boxes, uint32_t* tile_keys,
-                                cudaStream_t st) {
+                                const uint32_t* skeys, float4* s_sorted, float4* group_boxes, uint32_t* group_keys,
+                                uint32_t* gdesc, cudaStream_t st) {
     if (n_tiles <= 0) return cudaSuccess;
-    k_sample_tiles<<<nb256(n_tiles * 32), 256, 0, st>>>(S, n_tiles, samples, perm, skeys, s_sorted, tile_boxes,
-                                                        tile_keys); gvc::note_launch();
+    k_sample_tiles<<<nb256(n_tiles * 32), 256, 0, st>>>(S, n_tiles, samples, perm, skeys, s_sorted, group_boxes,
+                                                        group_keys, gdesc); gvc::note_launch();
     return cudaGetLastError();
 }
 

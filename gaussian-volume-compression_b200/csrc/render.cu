@@ -69,9 +69,15 @@ struct FwdVisitor {
     }
 };
 
+// Lane group of this lane in a tile with descriptor gd (see k_sample_tiles).
+__device__ __forceinline__ int lane_group(uint32_t gd, int lane) {
+    return (lane >= (int)(gd & 0xffu)) + (lane >= (int)((gd >> 8) & 0xffu)) + (lane >= (int)((gd >> 16) & 0xffu));
+}
+
 template <bool COUNT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_forward(const float4* __restrict__ s_sorted,
-                                                                 const float4* __restrict__ tile_boxes, int n_tiles,
+                                                                 const float4* __restrict__ group_boxes,
+                                                                 const uint32_t* __restrict__ gdesc, int n_tiles,
                                                                  const BvhNode* __restrict__ nodes,
                                                                  const GaussRec* __restrict__ recs,
                                                                  float* __restrict__ out_cells,
@@ -85,11 +91,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_forward(const float4* _
     if (tile >= n_tiles) return;
     const float4 sp = s_sorted[(int64_t)tile * 32 + lane];
     const int orig = __float_as_int(sp.w);
-    FwdVisitor vis{recs, s_batch[warp], sp.x, sp.y, sp.z, orig >= 0, 0.f, 0.f, 0, 0};
-    const float4 tlo = tile_boxes[2 * (int64_t)tile], thi = tile_boxes[2 * (int64_t)tile + 1];
-    int max_sp = 0;
-    const int st = warp_traverse(nodes, make_float3(tlo.x, tlo.y, tlo.z), make_float3(thi.x, thi.y, thi.z),
-                                 s_stack[warp], s_cand[warp], vis, max_sp);
+    const uint32_t gd = gdesc[tile];
+    const int ng = (int)(gd >> 24), mygroup = lane_group(gd, lane);
+    FwdVisitor vis{recs, s_batch[warp], sp.x, sp.y, sp.z, false, 0.f, 0.f, 0, 0};
+    TravCount tc;
+    int st = 0;
+    for (int g = 0; g < ng; g++) {
+        const int64_t slot = (int64_t)tile * kGroups + g;
+        const float4 tlo = group_boxes[2 * slot], thi = group_boxes[2 * slot + 1];
+        vis.valid = orig >= 0 && mygroup == g;
+        st |= warp_traverse(nodes, make_float3(tlo.x, tlo.y, tlo.z), make_float3(thi.x, thi.y, thi.z),
+                            s_stack[warp], s_cand[warp], vis, tc);
+    }
     if (orig >= 0) {
         float o, w;
         if (vis.W <= kWeightCutoff) {
@@ -112,7 +125,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_forward(const float4* _
         if (lane == 0) {
             atomicAdd(&stats[0], a);
             atomicAdd(&stats[1], b);
-            atomicMax(&stats[3], (unsigned long long)max_sp);
+            atomicMax(&stats[3], (unsigned long long)tc.max_sp);
+            atomicAdd(&stats[5], (unsigned long long)tc.leaves);
+            atomicAdd(&stats[6], (unsigned long long)tc.nodes);
         }
     }
 }
@@ -163,22 +178,33 @@ __device__ __forceinline__ bool pair_adjoint(const GaussParams& g, float4 sp, fl
 struct BwdGaussVisitor {
     const float4* __restrict__ s_sorted;
     const float4* __restrict__ s_grad;
+    const uint32_t* __restrict__ gdesc;
     GaussParams g;
     float acc[16];
     int npairs;
 
+    // leaf l = (tile l / kGroups, group l % kGroups): lanes [start, end) of the tile
+    __device__ __forceinline__ void load(int l, int lane, float4& sp, float4& sg, bool& in) const {
+        const int64_t t = l / kGroups;
+        const int gi = l % kGroups;
+        const uint32_t gd = __ldg(gdesc + t);
+        const int start = gi == 0 ? 0 : (int)((gd >> (8 * (gi - 1))) & 0xffu);
+        const int end = gi < 3 ? (int)((gd >> (8 * gi)) & 0xffu) : 32;
+        in = lane >= start && lane < end;
+        sp = __ldg(s_sorted + t * 32 + lane);
+        sg = __ldg(s_grad + t * 32 + lane);
+    }
+
     __device__ __forceinline__ void operator()(const int* c, int nb) {
         const int lane = threadIdx.x & 31;
-        int64_t t = c[0];
-        float4 sp = __ldg(s_sorted + t * 32 + lane), sg = __ldg(s_grad + t * 32 + lane);
+        float4 sp, sg;
+        bool in;
+        load(c[0], lane, sp, sg, in);
         for (int i = 0; i < nb; i++) {
             const float4 cs = sp, cg = sg;
-            if (i + 1 < nb) {
-                t = c[i + 1];
-                sp = __ldg(s_sorted + t * 32 + lane);
-                sg = __ldg(s_grad + t * 32 + lane);
-            }
-            npairs += pair_adjoint(g, cs, cg, acc) ? 1 : 0;
+            const bool cin = in;
+            if (i + 1 < nb) load(c[i + 1], lane, sp, sg, in);
+            if (cin) npairs += pair_adjoint(g, cs, cg, acc) ? 1 : 0;
         }
         __syncwarp();
     }
@@ -188,8 +214,8 @@ template <bool COUNT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_gauss(
     int P, const int32_t* __restrict__ gorder, const float* __restrict__ means, const float* __restrict__ values,
     const float* __restrict__ weights, const float* __restrict__ conics, const float4* __restrict__ boxes,
-    const float4* __restrict__ s_sorted, const float4* __restrict__ s_grad, const BvhNode* __restrict__ tnodes,
-    float* __restrict__ gacc, int* status, unsigned long long* stats) {
+    const float4* __restrict__ s_sorted, const float4* __restrict__ s_grad, const uint32_t* __restrict__ gdesc,
+    const BvhNode* __restrict__ tnodes, float* __restrict__ gacc, int* status, unsigned long long* stats) {
     __shared__ int s_stack[kWarpsPerBlock][kStackCap];
     __shared__ int s_cand[kWarpsPerBlock][kCandCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -199,6 +225,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_gauss(
     BwdGaussVisitor vis;
     vis.s_sorted = s_sorted;
     vis.s_grad = s_grad;
+    vis.gdesc = gdesc;
     vis.g.mx = __ldg(means + 3 * (int64_t)o);
     vis.g.my = __ldg(means + 3 * (int64_t)o + 1);
     vis.g.mz = __ldg(means + 3 * (int64_t)o + 2);
@@ -215,10 +242,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_gauss(
 #pragma unroll
     for (int k = 0; k < 16; k++) vis.acc[k] = 0.f;
     vis.npairs = 0;
-    int max_sp = 0;
+    TravCount tc;
     const int st = warp_traverse(tnodes, make_float3(vis.g.lo.x, vis.g.lo.y, vis.g.lo.z),
                                  make_float3(vis.g.hi.x, vis.g.hi.y, vis.g.hi.z), s_stack[warp], s_cand[warp], vis,
-                                 max_sp);
+                                 tc);
     const float tot = warp_transpose_reduce16(vis.acc);
     if (!(lane & 1)) {
         const int k = lane >> 1;  // value index held by this lane
@@ -230,7 +257,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_gauss(
         for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
         if (lane == 0) {
             atomicAdd(&stats[2], a);
-            atomicMax(&stats[4], (unsigned long long)max_sp);
+            atomicMax(&stats[4], (unsigned long long)tc.max_sp);
+            atomicAdd(&stats[7], (unsigned long long)tc.leaves);
+            atomicAdd(&stats[8], (unsigned long long)tc.nodes);
         }
     }
 }
@@ -285,9 +314,10 @@ struct BwdTileVisitor {
 
 template <bool COUNT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_tiles(
-    const float4* __restrict__ s_sorted, const float4* __restrict__ s_grad, const float4* __restrict__ tile_boxes,
-    int n_tiles, const BvhNode* __restrict__ gnodes, const GaussRec* __restrict__ recs,
-    const int32_t* __restrict__ gperm, float* __restrict__ gacc, int* status, unsigned long long* stats) {
+    const float4* __restrict__ s_sorted, const float4* __restrict__ s_grad, const float4* __restrict__ group_boxes,
+    const uint32_t* __restrict__ gdesc, int n_tiles, const BvhNode* __restrict__ gnodes,
+    const GaussRec* __restrict__ recs, const int32_t* __restrict__ gperm, float* __restrict__ gacc, int* status,
+    unsigned long long* stats) {
     __shared__ int s_stack[kWarpsPerBlock][kStackCap];
     __shared__ int s_cand[kWarpsPerBlock][kCandCap];
     __shared__ float4 s_batch[kWarpsPerBlock][32 * 5];
@@ -298,21 +328,32 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_tiles(
     vis.recs = recs;
     vis.gperm = gperm;
     vis.batch = s_batch[warp];
-    vis.sp = s_sorted[(int64_t)tile * 32 + lane];
-    vis.sg = s_grad[(int64_t)tile * 32 + lane];
+    const float4 sp = s_sorted[(int64_t)tile * 32 + lane];
+    const float4 sg = s_grad[(int64_t)tile * 32 + lane];
+    vis.sp = sp;
     vis.gacc = gacc;
     vis.npairs = 0;
-    const float4 tlo = tile_boxes[2 * (int64_t)tile], thi = tile_boxes[2 * (int64_t)tile + 1];
-    int max_sp = 0;
-    const int st = warp_traverse(gnodes, make_float3(tlo.x, tlo.y, tlo.z), make_float3(thi.x, thi.y, thi.z),
-                                 s_stack[warp], s_cand[warp], vis, max_sp);
+    const uint32_t gd = gdesc[tile];
+    const int ng = (int)(gd >> 24), mygroup = lane_group(gd, lane);
+    TravCount tc;
+    int st = 0;
+    for (int g = 0; g < ng; g++) {
+        const int64_t slot = (int64_t)tile * kGroups + g;
+        const float4 tlo = group_boxes[2 * slot], thi = group_boxes[2 * slot + 1];
+        // lanes outside the group see ok = 0 and contribute nothing
+        vis.sg = mygroup == g ? sg : make_float4(0.f, 0.f, 0.f, 0.f);
+        st |= warp_traverse(gnodes, make_float3(tlo.x, tlo.y, tlo.z), make_float3(thi.x, thi.y, thi.z),
+                            s_stack[warp], s_cand[warp], vis, tc);
+    }
     if (st && lane == 0) atomicOr(status, st);
     if (COUNT) {
         unsigned long long a = (unsigned long long)vis.npairs;
         for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
         if (lane == 0) {
             atomicAdd(&stats[2], a);
-            atomicMax(&stats[4], (unsigned long long)max_sp);
+            atomicMax(&stats[4], (unsigned long long)tc.max_sp);
+            atomicAdd(&stats[7], (unsigned long long)tc.leaves);
+            atomicAdd(&stats[8], (unsigned long long)tc.nodes);
         }
     }
 }
@@ -475,10 +516,12 @@ cudaError_t launch_forward(const FwdArgs& a, cudaStream_t st) {
     if (a.n_tiles <= 0) return cudaSuccess;
     if (a.count) {
         k_forward<true><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            a.s_sorted, a.tile_boxes, (int)a.n_tiles, a.gnodes, a.recs, a.out_cells, a.out_weights, a.status, a.stats);
+            a.s_sorted, a.tile_boxes, a.gdesc, (int)a.n_tiles, a.gnodes, a.recs, a.out_cells, a.out_weights, a.status,
+            a.stats);
     } else {
         k_forward<false><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            a.s_sorted, a.tile_boxes, (int)a.n_tiles, a.gnodes, a.recs, a.out_cells, a.out_weights, a.status, a.stats);
+            a.s_sorted, a.tile_boxes, a.gdesc, (int)a.n_tiles, a.gnodes, a.recs, a.out_cells, a.out_weights, a.status,
+            a.stats);
     }
     gvc::note_launch();
     return cudaGetLastError();
@@ -488,12 +531,12 @@ cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st) {
     if (a.P <= 0) return cudaSuccess;
     if (a.count) {
         k_backward_gauss<true><<<nblk(a.P, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_sorted, a.s_grad, a.tnodes,
-            a.gacc, a.status, a.stats);
+            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_sorted, a.s_grad, a.gdesc,
+            a.tnodes, a.gacc, a.status, a.stats);
     } else {
         k_backward_gauss<false><<<nblk(a.P, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_sorted, a.s_grad, a.tnodes,
-            a.gacc, a.status, a.stats);
+            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_sorted, a.s_grad, a.gdesc,
+            a.tnodes, a.gacc, a.status, a.stats);
     }
     gvc::note_launch();
     return cudaGetLastError();
@@ -503,10 +546,12 @@ cudaError_t launch_backward_tiles(const BwdArgs& a, cudaStream_t st) {
     if (a.n_tiles <= 0) return cudaSuccess;
     if (a.count) {
         k_backward_tiles<true><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            a.s_sorted, a.s_grad, a.tile_boxes, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc, a.status, a.stats);
+            a.s_sorted, a.s_grad, a.tile_boxes, a.gdesc, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc,
+            a.status, a.stats);
     } else {
         k_backward_tiles<false><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            a.s_sorted, a.s_grad, a.tile_boxes, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc, a.status, a.stats);
+            a.s_sorted, a.s_grad, a.tile_boxes, a.gdesc, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc,
+            a.status, a.stats);
     }
     gvc::note_launch();
     return cudaGetLastError();

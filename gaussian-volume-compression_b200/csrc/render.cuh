@@ -7,7 +7,8 @@ namespace gvc {
 
 struct FwdArgs {
     const float4* s_sorted;
-    const float4* tile_boxes;
+    const float4* tile_boxes;  // group boxes [n_tiles * kGroups]
+    const uint32_t* gdesc;     // [n_tiles]
     int64_t n_tiles;
     const BvhNode* gnodes;
     const GaussRec* recs;
@@ -29,9 +30,10 @@ struct BwdArgs {
     const float4* boxes;  // caller order, lo/hi
     const float4* s_sorted;
     const float4* s_grad;
-    const float4* tile_boxes;
+    const float4* tile_boxes;  // group boxes [n_tiles * kGroups]
+    const uint32_t* gdesc;     // [n_tiles]
     int64_t n_tiles;
-    const BvhNode* tnodes;  // sample-tile LBVH
+    const BvhNode* tnodes;  // sample-group LBVH
     const BvhNode* gnodes;  // Gaussian LBVH (atomic mode)
     const GaussRec* recs;   // LBVH order (atomic mode)
     float* gacc;            // [P][16] caller order
@@ -54,8 +56,8 @@ cudaError_t launch_gather_recs(int64_t P, const int32_t* perm, const float* mean
                                const float* weights, const float* conics, const float4* boxes, GaussRec* recs,
                                cudaStream_t st);
 cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples, const int32_t* perm,
-                                const uint32_t* skeys, float4* s_sorted, float4* tile_boxes, uint32_t* tile_keys,
-                                cudaStream_t st);
+                                const uint32_t* skeys, float4* s_sorted, float4* group_boxes, uint32_t* group_keys,
+                                uint32_t* gdesc, cudaStream_t st);
 cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float* out_cells,
                                 const float* out_weights, const float* gout, const float* gw, float4* s_grad,
                                 cudaStream_t st);

@@ -35,10 +35,17 @@ constexpr int kStackHeadroom = 128;
 
 // Returns 0, or kStatusStackOverflow if nodes had to be dropped (results invalid).
 // `visit(const int* cand, int nb)` is warp-collective and must end with __syncwarp().
+// Per-warp traversal counters (warp-uniform values).
+struct TravCount {
+    int max_sp = 0;   // deepest stack
+    int nodes = 0;    // internal nodes popped
+    int leaves = 0;   // leaves handed to the visitor
+};
+
 template <class Visitor>
 __device__ __forceinline__ int warp_traverse(const BvhNode* __restrict__ nodes, float3 qlo, float3 qhi,
                                              int* __restrict__ stack, int* __restrict__ cand, Visitor& visit,
-                                             int& max_sp) {
+                                             TravCount& tc) {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = lane_lt_mask();
     int status = 0;
@@ -51,6 +58,7 @@ __device__ __forceinline__ int warp_traverse(const BvhNode* __restrict__ nodes, 
         const int room = kStackCap - kStackHeadroom - sp;
         if (k > room) k = max(room, 1);
         const int base = sp - k;
+        tc.nodes += k;
         const int node = (lane < k) ? stack[base + lane] : 0;
         __syncwarp();
         sp = base;
@@ -72,6 +80,7 @@ __device__ __forceinline__ int warp_traverse(const BvhNode* __restrict__ nodes, 
         if (ll) cand[nc + __popc(mll & lt)] = (int)(cl & ~kLeafBit);
         if (lr) cand[nc + nll + __popc(mlr & lt)] = (int)(cr & ~kLeafBit);
         nc += nll + nlr;
+        tc.leaves += nll + nlr;
         if (sp + nil + nir > kStackCap) {
             status = kStatusStackOverflow;
         } else {
@@ -79,7 +88,7 @@ __device__ __forceinline__ int warp_traverse(const BvhNode* __restrict__ nodes, 
             if (ir) stack[sp + nil + __popc(mir & lt)] = (int)cr;
             sp += nil + nir;
         }
-        max_sp = max(max_sp, sp);
+        tc.max_sp = max(tc.max_sp, sp);
         __syncwarp();
         while (nc >= 32) {
             visit(cand + nc - 32, 32);

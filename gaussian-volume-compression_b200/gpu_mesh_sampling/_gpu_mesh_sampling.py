@@ -75,9 +75,10 @@ def sample_mesh(dims_arr, origin_arr, spacing_arr, val_arr, samp_arr):
     d_vals = torch.from_numpy(vals.reshape(-1).view(np.uint8)).to("cuda:%d" % dev)
     d_samp = _dev(samples, np.float32)
     d_out = torch.empty(n * vals.dtype.itemsize, dtype=torch.uint8, device="cuda:%d" % dev)
-    c.call("gvc_sample_uniform", _n.ptr(dims[:3].copy()), _n.ptr(origin[:3].copy()),
-           _n.ptr(spacing[:3].copy()), _n.ptr(d_vals), code, n, _n.ptr(d_samp), _n.ptr(d_out),
-           _stream(dev))
+    # host arrays must stay referenced until the call returns
+    h_dims, h_origin, h_spacing = dims[:3].copy(), origin[:3].copy(), spacing[:3].copy()
+    c.call("gvc_sample_uniform", _n.ptr(h_dims), _n.ptr(h_origin), _n.ptr(h_spacing), _n.ptr(d_vals), code, n,
+           _n.ptr(d_samp), _n.ptr(d_out), _stream(dev))
     out[:] = d_out.cpu().numpy().view(vals.dtype)
     return out
 

@@ -53,7 +53,9 @@ class GvcStats(ctypes.Structure):
                 ("bwd_contributing", ctypes.c_int64), ("max_stack_fwd", ctypes.c_int32),
                 ("max_stack_bwd", ctypes.c_int32), ("fwd_kernel_ms", ctypes.c_double),
                 ("bwd_kernel_ms", ctypes.c_double), ("fwd_kernel_calls", ctypes.c_int64),
-                ("bwd_kernel_calls", ctypes.c_int64)]
+                ("bwd_kernel_calls", ctypes.c_int64), ("fwd_leaf_hits", ctypes.c_int64),
+                ("fwd_node_visits", ctypes.c_int64), ("bwd_leaf_hits", ctypes.c_int64),
+                ("bwd_node_visits", ctypes.c_int64)]
 
 
 _lib = None

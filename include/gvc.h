@@ -62,6 +62,10 @@ typedef struct {
     double bwd_kernel_ms;     /* summed duration of the backward evaluation kernel         */
     int64_t fwd_kernel_calls; /* launches timed since the option was set                   */
     int64_t bwd_kernel_calls;
+    int64_t fwd_leaf_hits;    /* (tile, Gaussian) pairs evaluated by the forward            */
+    int64_t fwd_node_visits;  /* internal LBVH nodes popped by the forward traversal        */
+    int64_t bwd_leaf_hits;    /* (Gaussian or tile) leaves evaluated by the backward        */
+    int64_t bwd_node_visits;
 } gvc_stats;
 
 /* Context: owns the sample ordering, both LBVHs and all workspace (no per-call
