@@ -25,6 +25,7 @@ SOURCES = {
     "capi.cu": [],
     "prep.cu": ["--fmad=false"],
     "mesh.cu": ["--fmad=false"],
+    "noalloc.cu": [],
 }
 
 

@@ -130,6 +130,21 @@ int gvc_sample_tets(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, con
                     const double* values, int64_t N, const float* samples, double* out, int64_t* cell_ids,
                     void* stream);
 
+/* No counterpart in the reference.  Tetrahedral sampling for callers that cannot
+   allocate device memory (their memory belongs to another allocator, or cudaMalloc's
+   device-wide synchronisation is unacceptable where they call).  Same inputs, outputs
+   and results as gvc_sample_tets, but no context and no allocation: the scratch is one
+   static device array of about 6.4 MB in every device that loads the library, which
+   limits the mesh to C <= 32768 cells (larger meshes are rejected with
+   GVC_ERR_CAPACITY and a message in errbuf).  The first call on a device looks up the
+   array's device address and should come before any stream capture on that device.
+   Calls share the array: calls that overlap on the GPU race, so issue them one after
+   another.  Samples are traversed in the caller's order; the call waits for `stream`
+   to report a traversal overflow.  errbuf (host, may be NULL) receives a message. */
+int gvc_sample_tets_static(int64_t npts, const float* pts, int64_t C, const int32_t* conn4, const double* values,
+                           int64_t N, const float* samples, double* out, int64_t* cell_ids, void* stream,
+                           char* errbuf, int64_t errbuf_len);
+
 /* Test hook: builds the LBVH over n boxes [n,6] (lo xyz, hi xyz) exactly as the
    forward does over Gaussian AABBs, and copies the result out (device pointers):
    keys_sorted [n] uint32, perm [n] int32, left/right [n-1] int32 (leaf i encoded as
