@@ -4,7 +4,7 @@
 #include <stdint.h>
 #include <string>
 
-#include "../../include/gvc.h"
+#include "gvc.h"
 
 namespace gvc {
 

@@ -28,6 +28,19 @@ constexpr int kWarpsPerBlock = 4;
 // --------------------------------------------------------------------------------
 // Forward
 // --------------------------------------------------------------------------------
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// -0.5 * log2(e): folds the -1/2 of the power (forward.cu:234) and the change of base
+// of the exponential into the staged conic, so the power arrives in base 2.
+constexpr float kHalfLog2e = -0.72134752044448170368f;
+// The power floor -14 (forward.cu:235) in base 2.
+constexpr float kLog2Floor = -20.197570572173914f;
+
+template <bool COUNT>
 struct FwdVisitor {
     const GaussRec* __restrict__ recs;
     float4* batch;  // shared [32 * 5]
@@ -39,30 +52,49 @@ struct FwdVisitor {
     __device__ __forceinline__ void operator()(const int* c, int nb) {
         const int lane = threadIdx.x & 31;
         if (lane < nb) {
+            // stage one record per lane; the conic becomes base-2 power coefficients with
+            // the off-diagonal entries doubled (symmetric quadratic form in 9 operations)
             const float4* rp = reinterpret_cast<const float4*>(recs + c[lane]);
-            float4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2), r3 = __ldg(rp + 3), r4 = __ldg(rp + 4);
+            const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2), r3 = __ldg(rp + 3),
+                         r4 = __ldg(rp + 4);
             batch[lane * 5 + 0] = r0;
-            batch[lane * 5 + 1] = r1;
-            batch[lane * 5 + 2] = r2;
+            batch[lane * 5 + 1] = make_float4(kHalfLog2e * r1.x, 2.f * kHalfLog2e * r1.y, 2.f * kHalfLog2e * r1.z,
+                                              kHalfLog2e * r1.w);
+            batch[lane * 5 + 2] = make_float4(2.f * kHalfLog2e * r2.x, kHalfLog2e * r2.y, r2.z, 0.f);
             batch[lane * 5 + 3] = r3;
             batch[lane * 5 + 4] = r4;
         }
         __syncwarp();
-        if (valid) {
-            for (int g = 0; g < nb; g++) {
-                const float4 r3 = batch[g * 5 + 3], r4 = batch[g * 5 + 4];
-                if (!(r3.x <= x && x <= r4.x && r3.y <= y && y <= r4.y && r3.z <= z && z <= r4.z)) continue;
+        // Four Gaussians per step, branch-free inside the step: four independent
+        // dependency chains per lane; a step is skipped only when no lane of the warp is
+        // inside any of the four boxes.
+        for (int g0 = 0; g0 < nb; g0 += 4) {
+            bool in[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int g = g0 + j;
+                in[j] = false;
+                if (g < nb) {
+                    const float4 r3 = batch[g * 5 + 3], r4 = batch[g * 5 + 4];
+                    in[j] = valid && r3.x <= x && x <= r4.x && r3.y <= y && y <= r4.y && r3.z <= z && z <= r4.z;
+                }
+            }
+            if (!__any_sync(0xffffffffu, in[0] | in[1] | in[2] | in[3])) continue;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int g = min(g0 + j, nb - 1);
                 const float4 r0 = batch[g * 5 + 0], r1 = batch[g * 5 + 1], r2 = batch[g * 5 + 2];
-                ncand++;
                 const float dx = x - r0.x, dy = y - r0.y, dz = z - r0.z;
-                const float q = dx * (r1.x * dx + r1.y * dy + r1.z * dz) + dy * (r1.y * dx + r1.w * dy + r2.x * dz) +
-                                dz * (r1.z * dx + r2.x * dy + r2.y * dz);
-                const float p = -0.5f * q;
-                if (p < kPowerFloor || p > 0.0f) continue;
-                const float wt = r0.w * __expf(p);
+                const float p2 = dx * fmaf(r1.x, dx, fmaf(r1.y, dy, r1.z * dz)) + dy * fmaf(r1.w, dy, r2.x * dz) +
+                                 dz * (r2.y * dz);
+                const bool c = in[j] && p2 >= kLog2Floor && p2 <= 0.0f;
+                const float wt = c ? r0.w * ex2_approx(p2) : 0.0f;
                 W += wt;
-                V += wt * r2.z;
-                ncontrib++;
+                V = fmaf(wt, r2.z, V);
+                if (COUNT) {
+                    ncand += in[j] ? 1 : 0;
+                    ncontrib += c ? 1 : 0;
+                }
             }
         }
         __syncwarp();
@@ -93,7 +125,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_forward(const float4* _
     const int orig = __float_as_int(sp.w);
     const uint32_t gd = gdesc[tile];
     const int ng = (int)(gd >> 24), mygroup = lane_group(gd, lane);
-    FwdVisitor vis{recs, s_batch[warp], sp.x, sp.y, sp.z, false, 0.f, 0.f, 0, 0};
+    FwdVisitor<COUNT> vis{recs, s_batch[warp], sp.x, sp.y, sp.z, false, 0.f, 0.f, 0, 0};
     TravCount tc;
     int st = 0;
     for (int g = 0; g < ng; g++) {
@@ -175,6 +207,9 @@ __device__ __forceinline__ bool pair_adjoint(const GaussParams& g, float4 sp, fl
 // --------------------------------------------------------------------------------
 // Backward, deterministic Gaussian-owned segmented reduction.
 // --------------------------------------------------------------------------------
+// Gaussian-owned visitor: the warp's lanes are the samples of each candidate group; two
+// groups are evaluated per step (their loads issued together, two independent
+// dependency chains per lane).
 struct BwdGaussVisitor {
     const float4* __restrict__ s_sorted;
     const float4* __restrict__ s_grad;
@@ -197,14 +232,14 @@ struct BwdGaussVisitor {
 
     __device__ __forceinline__ void operator()(const int* c, int nb) {
         const int lane = threadIdx.x & 31;
-        float4 sp, sg;
-        bool in;
-        load(c[0], lane, sp, sg, in);
-        for (int i = 0; i < nb; i++) {
-            const float4 cs = sp, cg = sg;
-            const bool cin = in;
-            if (i + 1 < nb) load(c[i + 1], lane, sp, sg, in);
-            if (cin) npairs += pair_adjoint(g, cs, cg, acc) ? 1 : 0;
+        for (int i = 0; i < nb; i += 2) {
+            float4 sp0, sg0, sp1, sg1;
+            bool in0, in1;
+            load(c[i], lane, sp0, sg0, in0);
+            load(c[min(i + 1, nb - 1)], lane, sp1, sg1, in1);
+            in1 = in1 && (i + 1 < nb);
+            if (in0) npairs += pair_adjoint(g, sp0, sg0, acc) ? 1 : 0;
+            if (in1) npairs += pair_adjoint(g, sp1, sg1, acc) ? 1 : 0;
         }
         __syncwarp();
     }
@@ -226,6 +261,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_gauss(
     vis.s_sorted = s_sorted;
     vis.s_grad = s_grad;
     vis.gdesc = gdesc;
+
     vis.g.mx = __ldg(means + 3 * (int64_t)o);
     vis.g.my = __ldg(means + 3 * (int64_t)o + 1);
     vis.g.mz = __ldg(means + 3 * (int64_t)o + 2);

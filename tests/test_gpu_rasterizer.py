@@ -5,8 +5,9 @@ Tolerances (FP32 kernels vs the FP64 oracle):
   * preprocess conics: bit-exact; AABBs: bit-exact except <= 1 ulp where CUDA's and the
     host's double log differ (<= 0.1% of boxes);
   * LBVH keys / permutation / topology / node boxes, sample order: bit-exact;
-  * forward given the same conics and boxes: |d out| <= 2e-5, |d outw| <= 2e-5 outw;
-  * forward vs the full FP64 pipeline: relative error <= 1e-4 (out and outw);
+  * forward given the same conics and boxes: |d out| <= 2e-5, |d outw| <= 2e-5 outw, plus
+    an allowance for pairs at the -14 power floor (see FLOOR_PAIR);
+  * forward vs the full FP64 pipeline: relative error <= 1e-4 (out and outw), same allowance;
   * backward given the same inputs: max |d grad| <= 1e-4 max |grad| per field (5e-4 for
     the covariance adjoint);
   * gradients vs FP64 central finite differences: |an - fd| <= 1e-3 max(|fd|, 1e-3).
@@ -122,15 +123,22 @@ def run_forward(dev, means, scales, rots, values, weights, samples, use_gaussian
     return out, outw, conics
 
 
+# A pair whose power lies within rounding of the -14 floor (forward.cu:235) may be kept by
+# one side and dropped by the other; its contribution is w e^-14 <= 8.4e-7.  Every sample
+# is allowed two such pairs: |dW| <= rtol W + 2e-6 and |d out| <= atol + 2e-6 / W.
+FLOOR_PAIR = 2e-6
+
+
 def compare_forward(out, outw, ref_out, ref_w, atol_out, rtol_w):
-    near = np.abs(ref_w - 0.01) <= 1e-5 * 0.01 + 1e-9
+    near = np.abs(ref_w - 0.01) <= 1e-5 * 0.01 + FLOOR_PAIR
     ok = ~near
     vo, vr = out[ok] != -1, ref_out[ok] != -1
     assert np.array_equal(vo, vr)
     both = ok.copy()
     both[ok] = vo
-    err_o = np.abs(out[both] - ref_out[both]).max(initial=0)
-    err_w = (np.abs(outw[both] - ref_w[both]) / ref_w[both]).max(initial=0)
+    W = ref_w[both]
+    err_o = (np.abs(out[both] - ref_out[both]) - FLOOR_PAIR / W).max(initial=0)
+    err_w = ((np.abs(outw[both] - W) - FLOOR_PAIR) / W).max(initial=0)
     assert err_o <= atol_out, err_o
     assert err_w <= rtol_w, err_w
     return err_o, err_w
