@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="large", choices=list(CONFIGS))
     p.add_argument("--bwd-mode", default="auto", choices=["auto", "deterministic", "atomic"])
+    p.add_argument("--eval-path", default="plain", choices=["plain", "tensor_core", "plain_cta"])
     p.add_argument("--use-gaussian-bvh", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -222,6 +223,7 @@ def run_ours(args):
     zeros_w = torch.zeros(S, device=dev)
     ugb = bool(args.use_gaussian_bvh)
     _C.set_backward_mode(args.bwd_mode)
+    _C.set_eval_path(args.eval_path)
     bounds = (0.0, 0.0, 0.0, 1.0, 1.0, 1.0)
 
     def step():
@@ -346,7 +348,7 @@ def run_ours(args):
         line = {"metric": METRIC, "value": ms, "unit": "ms/step", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": desc, "P": P, "S_per_gpu": S, "path": "plain FP32",
+                "config": {"workload": desc, "P": P, "S_per_gpu": S, "path": args.eval_path,
                            "backward": args.bwd_mode, "use_gaussian_bvh": ugb,
                            "l2": "inputs larger than L2 (samples %d MB, Gaussian records %d MB)" %
                                  (S * 12 // 2**20, P * 80 // 2**20),

@@ -26,6 +26,7 @@ SOURCES = {
     "prep.cu": ["--fmad=false"],
     "mesh.cu": ["--fmad=false"],
     "noalloc.cu": [],
+    "cta.cu": [],
 }
 
 

@@ -189,6 +189,12 @@ def set_backward_mode(mode, device=None):
     set_option(_n.OPT_BWD_MODE, {"auto": 0, "deterministic": 1, "atomic": 2}[mode], device)
 
 
+def set_eval_path(path, device=None):
+    """Forward exponent: 'plain' (default, warp per 32-sample tile), 'tensor_core'
+    (tcgen05 BF16 split MMA, CTA per 128 samples) or 'plain_cta' (same CTA structure, FP32)."""
+    set_option(_n.OPT_EVAL_PATH, {"plain": 0, "tensor_core": 1, "plain_cta": 2}[path], device)
+
+
 def set_count_pairs(on, device=None):
     set_option(_n.OPT_COUNT_PAIRS, 1 if on else 0, device)
 

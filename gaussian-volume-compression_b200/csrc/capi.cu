@@ -185,7 +185,7 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
                           &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds};
         for (DevBuf* b : bufs) b->release();
     }
-    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->s_grad, &c->grec, &c->gtmp,
+    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->s_grad, &c->grec, &c->gtmp,
                       &c->m_out_sorted, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
     for (DevBuf* b : bufs) b->release();
     if (c->d_status) cudaFree(c->d_status);
@@ -211,7 +211,7 @@ int gvc_set_option(gvc_ctx* ctx, int option, int value) {
             ctx->bwd_mode = value;
             return GVC_OK;
         case GVC_OPT_EVAL_PATH:
-            if (value != 0) return fail(ctx, GVC_ERR_UNSUPPORTED, "only the plain FP32 exponent path is built");
+            if (value < 0 || value > 2) return fail(ctx, GVC_ERR_ARG, "eval path must be 0, 1 or 2");
             ctx->eval_path = value;
             return GVC_OK;
         case GVC_OPT_COUNT_PAIRS:
@@ -283,6 +283,12 @@ int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int 
                  "sample tiles");
         GVC_CUDA(lbvh_hierarchy(ctx->tiles, slots_g, ctx->tile_keys.as<uint32_t>(), ctx->tile_boxes.as<float4>(), st),
                  "sample-group LBVH");
+        const int64_t n_blocks = (S + 127) / 128;
+        GVC_CUDA(ctx->blk_desc.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc");
+        GVC_CUDA(ctx->blk_boxes.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes");
+        GVC_CUDA(launch_sample_blocks(S, ctx->s_sorted.as<float4>(), ctx->s_sort.keys.as<uint32_t>(),
+                                      ctx->blk_desc.as<uint2>(), ctx->blk_boxes.as<float4>(), st),
+                 "sample blocks");
     }
     ctx->samples_ready = true;
     tm.mark();
@@ -341,7 +347,23 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
     fa.stats = ctx->d_stats;
     fa.count = ctx->count_pairs != 0;
     const int tk = timer_begin(ctx, st, 0);
-    GVC_CUDA(launch_forward(fa, st), "forward");
+    if (ctx->eval_path == 0) {
+        GVC_CUDA(launch_forward(fa, st), "forward");
+    } else {
+        CtaArgs ca;
+        ca.s_sorted = ctx->s_sorted.as<float4>();
+        ca.S = ctx->S;
+        ca.bdesc = ctx->blk_desc.as<uint2>();
+        ca.bboxes = ctx->blk_boxes.as<float4>();
+        ca.gnodes = ctx->gbvh.nodes.as<BvhNode>();
+        ca.recs = ctx->grec.as<GaussRec>();
+        ca.out_cells = out_cells;
+        ca.out_weights = out_weights;
+        ca.status = ctx->d_status;
+        ca.stats = ctx->d_stats;
+        ca.count = ctx->count_pairs != 0;
+        GVC_CUDA(launch_forward_cta(ca, ctx->eval_path == 1, st), "forward (CTA)");
+    }
     timer_end(ctx, st, tk);
     tm.mark();
     ctx->P = P;
@@ -532,6 +554,14 @@ int gvc_debug_preprocess(gvc_ctx* ctx, int64_t P, const float* means3D, const fl
              "preprocess");
     if (aabbs) k_f4_to_boxes6<<<nb(P, 256), 256, 0, st>>>(P, sc->tmp_boxes.as<float4>(), aabbs); gvc::note_launch();
     GVC_CUDA(cudaGetLastError(), "debug preprocess");
+    return GVC_OK;
+}
+
+int gvc_debug_tc_gemm(gvc_ctx* ctx, const void* A, const void* B, int N, float* D, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (N < 32 || N > 256 || N % 32) return fail(ctx, GVC_ERR_ARG, "N must be a multiple of 32 in [32, 256]");
+    if (!A || !B || !D) return fail(ctx, GVC_ERR_ARG, "null pointer");
+    GVC_CUDA(launch_tc_gemm_test(A, B, N, D, ctx->d_status, (cudaStream_t)stream), "tc gemm");
     return GVC_OK;
 }
 

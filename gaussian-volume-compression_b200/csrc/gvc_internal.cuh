@@ -113,6 +113,8 @@ struct gvc_ctx {
     gvc::DevBuf tile_keys;  // [n_tiles * kGroups] uint32 Morton key of each group's first sample
     gvc::DevBuf tile_gdesc; // [n_tiles] group starts: bytes 0..2 = start lane of groups 1..3
                             // (32 if unused), byte 3 = number of groups
+    gvc::DevBuf blk_desc;   // [ceil(S/128)] uint2 block-group descriptors (CTA kernels)
+    gvc::DevBuf blk_boxes;  // [ceil(S/128) * 8] block-group boxes, 2 x float4
     gvc::DevBuf s_grad;     // [n_tiles*32] float4 (out, outw, dL_dout, dL_doutw) for the backward
     gvc::Lbvh s_sort;       // sample sort (keys/perm only)
     gvc::Lbvh tiles;        // tile LBVH

@@ -43,6 +43,25 @@ struct BwdArgs {
 };
 
 cudaError_t launch_forward(const FwdArgs& a, cudaStream_t st);
+
+// cta.cu: CTA-level forward on 128-sample blocks (tensor-core or SIMT exponent)
+struct CtaArgs {
+    const float4* s_sorted;
+    int64_t S;
+    const uint2* bdesc;    // [n_blocks] block-group descriptors
+    const float4* bboxes;  // [n_blocks * 8] block-group boxes (lo, hi)
+    const BvhNode* gnodes;
+    const GaussRec* recs;
+    float* out_cells;
+    float* out_weights;
+    int* status;
+    unsigned long long* stats;
+    bool count;
+};
+cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32_t* skeys, uint2* bdesc,
+                                 float4* bboxes, cudaStream_t st);
+cudaError_t launch_forward_cta(const CtaArgs& a, bool tc, cudaStream_t st);
+cudaError_t launch_tc_gemm_test(const void* A, const void* B, int N, float* D, int* status, cudaStream_t st);
 cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st);
 cudaError_t launch_backward_tiles(const BwdArgs& a, cudaStream_t st);
 cudaError_t launch_finalize(int64_t P, const float* gacc, const float* scales, const float* rots, const float* conics,

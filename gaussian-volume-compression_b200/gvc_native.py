@@ -44,6 +44,7 @@ _SIGNATURES = {
     "gvc_debug_lbvh": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "gvc_debug_preprocess": [_vp, _i64, _vp, _vp, _vp, _vp, _f32, _vp, _vp, _vp],
     "gvc_debug_sample_order": [_vp, _vp, _vp, _vp],
+    "gvc_debug_tc_gemm": [_vp, _vp, _vp, _int, _vp, _vp],
     "gvc_sample_tets_static": [_i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i64],
 }
 _RESTYPES = {"gvc_ctx_destroy": None, "gvc_last_error": ctypes.c_char_p, "gvc_launch_count": ctypes.c_int64}

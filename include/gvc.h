@@ -45,8 +45,11 @@ typedef enum {
                                    use_gaussian_bvh != 0 -> sample-tile traversal with warp
                                    pre-reduction + FP32 atomics (mirrors backward.cu:339-559);
                                1 = always deterministic, 2 = always atomic                */
-    GVC_OPT_EVAL_PATH = 3,  /* 0 = plain FP32 CUDA-core exponent (default),
-                               1 = tensor-core (tcgen05) BF16 split exponent                */
+    GVC_OPT_EVAL_PATH = 3,  /* forward evaluation kernel:
+                               0 = plain FP32 exponent, one warp per 32-sample tile (default),
+                               1 = tensor-core exponent: tcgen05 BF16 3-way split MMA into TMEM,
+                                   one CTA per 128-sample block,
+                               2 = plain FP32 exponent with the CTA structure of path 1     */
     GVC_OPT_COUNT_PAIRS = 4,/* 1 = record per-call pair counts (gvc_get_stats)            */
     GVC_OPT_TIME_KERNELS = 5 /* 1 = time the evaluation kernels with CUDA events on the
                                 caller's stream (gvc_get_stats)                          */
@@ -157,6 +160,11 @@ int gvc_debug_lbvh(gvc_ctx* ctx, int64_t n, const float* boxes, uint32_t* keys_s
    conics [6P] and AABBs [P,6] in the caller's order. */
 int gvc_debug_preprocess(gvc_ctx* ctx, int64_t P, const float* means3D, const float* scales, const float* rotations,
                          const float* weights, float scale_modifier, float* conics, float* aabbs, void* stream);
+
+/* Test hook: D[128 x N] = A[128 x 16] * B[N x 16]^T with BF16 inputs and FP32 output on
+   the tensor cores (tcgen05.mma, one CTA); N a multiple of 32 in [32, 256]; row-major
+   device arrays.  No counterpart in the reference. */
+int gvc_debug_tc_gemm(gvc_ctx* ctx, const void* A, const void* B, int N, float* D, void* stream);
 
 /* Test hook: the sample ordering of the last gvc_build_bvh: perm [S] int32 (sorted
    position -> caller index) and keys [S] uint32. */

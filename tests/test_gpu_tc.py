@@ -1,0 +1,99 @@
+"""Tensor-core (tcgen05) path: the MMA building block through the C ABI, and the CTA
+forward with the tensor-core exponent (and its FP32 SIMT twin) against the oracle.
+
+Tolerances: the GEMM hook is exact on small integers and within 1e-6 (relative to the
+row norm) on random BF16 data; the plain CTA forward meets the plain tolerance (2e-5);
+the tensor-core forward is checked at 1e-4 (the power is a dot product of ~100-sized
+terms accumulated in FP32 on the tensor cores) with the same -14-floor allowance."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import gvc_native
+from test_gpu_rasterizer import T, compare_forward, gpu_preprocess, run_forward
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16(a, dev):
+    return torch.tensor(a, dtype=torch.float32).to(torch.bfloat16).to(dev)
+
+
+@pytest.mark.parametrize("N", [32, 64, 128, 256])
+def test_tc_gemm_exact_on_integers(cuda, N):
+    rng = np.random.default_rng(N)
+    A = rng.integers(-4, 5, (128, 16)).astype(np.float32)
+    B = rng.integers(-4, 5, (N, 16)).astype(np.float32)
+    ctx = gvc_native.Context()
+    dA, dB = bf16(A, cuda), bf16(B, cuda)
+    D = torch.empty(128 * N, device=cuda)
+    ctx.call("gvc_debug_tc_gemm", gvc_native.ptr(dA), gvc_native.ptr(dB), N, gvc_native.ptr(D),
+             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    ctx.sync_status(torch.cuda.current_stream().cuda_stream)
+    np.testing.assert_array_equal(D.cpu().numpy().reshape(128, N), A @ B.T)
+
+
+def test_tc_gemm_random_bf16(cuda):
+    rng = np.random.default_rng(5)
+    A = rng.normal(size=(128, 16)).astype(np.float32)
+    B = rng.normal(size=(64, 16)).astype(np.float32)
+    dA, dB = bf16(A, cuda), bf16(B, cuda)
+    A64 = dA.float().cpu().numpy().astype(np.float64)
+    B64 = dB.float().cpu().numpy().astype(np.float64)
+    ctx = gvc_native.Context()
+    D = torch.empty(128 * 64, device=cuda)
+    ctx.call("gvc_debug_tc_gemm", gvc_native.ptr(dA), gvc_native.ptr(dB), 64, gvc_native.ptr(D),
+             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    ctx.sync_status(torch.cuda.current_stream().cuda_stream)
+    ref = A64 @ B64.T
+    scale = np.abs(A64).sum(1)[:, None] * np.abs(B64).max()
+    assert (np.abs(D.cpu().numpy().reshape(128, 64) - ref) / scale).max() <= 1e-6
+
+
+def run_path(dev, case, path):
+    from bvh_diff_gaussian_rasterization import _C
+    _C.set_eval_path(path)
+    try:
+        return run_forward(dev, *case)
+    finally:
+        _C.set_eval_path("plain")
+
+
+@pytest.fixture(scope="module")
+def case(cuda, orc):
+    means, scales, rots, values, weights = orc.mixture_small(seed=0, P=4096)
+    return means, scales, rots, values, weights, orc.grid_centres(64)
+
+
+@pytest.mark.parametrize("path,tol", [("plain_cta", 2e-5), ("tensor_core", 1e-4)])
+def test_cta_forward_matches_oracle(cuda, orc, case, path, tol):
+    means, scales, rots, values, weights, samples = case
+    out, outw, conics = run_path(cuda, case, path)
+    out, outw = out.cpu().numpy(), outw.cpu().numpy()
+    gc = conics.cpu().numpy().reshape(-1, 6)
+    _, gb = gpu_preprocess(gvc_native.Context(), cuda, means, scales, rots, weights)
+    ro, rw = orc.forward(means, values, weights, gc.astype(np.float64), gb, samples)
+    e_same = compare_forward(out, outw, ro, rw, tol, tol)
+    _, c64, bb = orc.preprocess(means, scales, rots, weights)
+    to, tw = orc.forward(means, values, weights, c64, bb, samples)
+    e64 = compare_forward(out, outw, to, tw, 1e-4, 1e-4)
+    print("%s: error vs oracle (same conics) out %.2e outw %.2e; vs FP64 pipeline out %.2e outw %.2e"
+          % (path, e_same[0], e_same[1], e64[0], e64[1]))
+
+
+def test_tensor_core_forward_large_clustered(cuda, orc):
+    """Scaled large-evaluation workload: the tensor-core field agrees with the plain one."""
+    means, scales, rots, values, weights, samples = orc.mixture_large(seed=3, P=200_000, S=1_000_000)
+    case = (means, scales, rots, values, weights, samples)
+    a = [x.cpu().numpy() for x in run_path(cuda, case, "plain")[:2]]
+    b = [x.cpu().numpy() for x in run_path(cuda, case, "tensor_core")[:2]]
+    c = [x.cpu().numpy() for x in run_path(cuda, case, "plain_cta")[:2]]
+    for other, tol in ((c, 2e-5), (b, 1e-4)):
+        near = np.abs(a[1] - 0.01) <= 1e-6 + 4e-6
+        ok = ~near
+        assert np.array_equal(a[0][ok] == -1, other[0][ok] == -1)
+        v = ok & (a[0] != -1)
+        assert ((np.abs(other[1][v] - a[1][v]) - 4e-6) / a[1][v]).max() <= tol
+        assert (np.abs(other[0][v] - a[0][v]) - 4e-6 / a[1][v]).max() <= tol
