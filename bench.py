@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="large", choices=list(CONFIGS))
     p.add_argument("--bwd-mode", default="auto", choices=["auto", "deterministic", "atomic"])
-    p.add_argument("--eval-path", default="plain", choices=["plain", "tensor_core", "plain_cta"])
+    p.add_argument("--eval-path", default="plain", choices=["plain", "tensor_core", "plain_tile"])
     p.add_argument("--use-gaussian-bvh", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -168,6 +168,34 @@ def cpu_baseline(means, scales, rots, values, weights, samples, sizes=(250_000, 
                       "(%.2f s, %.2f s), linearly extrapolated to the full step" %
                       (threads, sizes[0], sizes[1], samples.shape[0], means.shape[0], t[0], t[1]),
             "extrapolated": True}
+
+
+def fp64_errors(means, scales, rots, values, weights, samples, paths, n_sub=50_000, seed=7):
+    """Checker, outside every timed region: each path's forward (cells = V/W and W) against
+    the oracle's FP64 evaluation of the same conics at a random subset of points.  Reports
+    the largest and the 99.99th-percentile relative error over points the reference marks
+    valid, and the share of points above 1e-4.  Points whose W lies within 1e-6 of the 0.01
+    validity threshold are left out (either answer is within rounding)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(samples.shape[0], n_sub, replace=False))
+    sub = samples[idx]
+    _, _, bb = oracle.preprocess(means, scales, rots, weights)
+    res = {"points": int(n_sub), "reference": "oracle FP64 evaluation (C) of the path's own FP32 conics"}
+    for name, d in paths.items():
+        ro, rw = oracle.forward(means, values, weights, d["conics"].astype(np.float64), bb, sub)
+        o, w = d["out"][idx].astype(np.float64), d["outw"][idx].astype(np.float64)
+        ok = (ro != -1) & (np.abs(rw - 0.01) > 1e-6)
+        e_out = np.abs(o[ok] - ro[ok]) / np.maximum(np.abs(ro[ok]), 1e-6)
+        e_w = np.abs(w[ok] - rw[ok]) / rw[ok]
+        mism = int(((o != -1) != (ro != -1))[np.abs(rw - 0.01) > 1e-6].sum())
+        res[name] = {"cells_max_rel": float(e_out.max()) if e_out.size else 0.0,
+                     "cells_p9999_rel": float(np.quantile(e_out, 0.9999)) if e_out.size else 0.0,
+                     "weights_max_rel": float(e_w.max()) if e_w.size else 0.0,
+                     "share_above_1e-4": float((np.maximum(e_out, e_w) > 1e-4).mean()) if e_out.size else 0.0,
+                     "validity_mismatches": mism, "valid_points": int(ok.sum())}
+    return res
 
 
 def run_reference(args):
@@ -340,9 +368,43 @@ def run_ours(args):
         e2e = {"value": e2e_ms, "unit": "ms/step", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4,
                "steps": n_e2e, "path": "GaussianRasterizer (autograd) + masked L1 + loss.item()"}
 
+    # the two evaluation paths side by side: full step time and forward outputs (kept on the
+    # host for the FP64 comparison below)
+    paths = {}
+    if not args.profile:
+        for path in ("plain", "tensor_core"):
+            _C.set_eval_path(path)
+            for _ in range(2):
+                step()
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            b0.record(stream)
+            for _ in range(args.steps):
+                step()
+            b1.record(stream)
+            torch.cuda.synchronize()
+            pm = gvc_dist.max_over_ranks(b0.elapsed_time(b1) / args.steps, dev)
+            _C.build_bvh(d_samples, False, ugb)
+            o, ow, cn = _C.rasterize_gaussians(d_means, d_scales, d_rots, d_values, d_weights, 1.0, *bounds, -1.0,
+                                               ugb, False)
+            paths[path] = {"ms_per_step": pm, "out": o.cpu().numpy(), "outw": ow.cpu().numpy(),
+                           "conics": cn.cpu().numpy().reshape(-1, 6)}
+        _C.set_eval_path(args.eval_path)
+        _C.check_status()
+
     cpu = None
+    fp64 = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
         cpu = cpu_baseline(means, scales, rots, values, weights, samples)
+        fp64 = fp64_errors(means, scales, rots, values, weights, samples, paths)
+    tc_vs_plain = None
+    if paths:
+        tc_vs_plain = {"plain_ms_per_step": paths["plain"]["ms_per_step"],
+                       "tensor_core_ms_per_step": paths["tensor_core"]["ms_per_step"],
+                       "speedup_tc_over_plain": paths["plain"]["ms_per_step"] / paths["tensor_core"]["ms_per_step"],
+                       "fp64_error": fp64}
 
     if rank == 0:
         line = {"metric": METRIC, "value": ms, "unit": "ms/step", "n_gpus": world, "steps": args.steps,
@@ -354,7 +416,7 @@ def run_ours(args):
                                  (S * 12 // 2**20, P * 80 // 2**20),
                            "parallelism": "samples sharded per rank, NCCL all-reduce of gradients" if world > 1
                            else "single GPU"},
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e, "tc_vs_plain": tc_vs_plain,
                 "gpu_launches": int(launches), "gpu_launches_per_step": launches / args.steps}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -190,9 +190,9 @@ def set_backward_mode(mode, device=None):
 
 
 def set_eval_path(path, device=None):
-    """Forward exponent: 'plain' (default, warp per 32-sample tile), 'tensor_core'
-    (tcgen05 BF16 split MMA, CTA per 128 samples) or 'plain_cta' (same CTA structure, FP32)."""
-    set_option(_n.OPT_EVAL_PATH, {"plain": 0, "tensor_core": 1, "plain_cta": 2}[path], device)
+    """Forward kernel: 'plain' (default: FP32, CTA per 128 samples), 'tensor_core'
+    (tcgen05 BF16 split exponent, same pipeline) or 'plain_tile' (FP32, warp per 32 samples)."""
+    set_option(_n.OPT_EVAL_PATH, {"plain": 0, "tensor_core": 1, "plain_tile": 2}[path], device)
 
 
 def set_count_pairs(on, device=None):

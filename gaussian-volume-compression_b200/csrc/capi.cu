@@ -347,7 +347,7 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
     fa.stats = ctx->d_stats;
     fa.count = ctx->count_pairs != 0;
     const int tk = timer_begin(ctx, st, 0);
-    if (ctx->eval_path == 0) {
+    if (ctx->eval_path == 2) {
         GVC_CUDA(launch_forward(fa, st), "forward");
     } else {
         CtaArgs ca;
@@ -510,6 +510,35 @@ int gvc_sample_tets(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, con
     GVC_CUDA(launch_sample_tets(N, samples, sc->msamp.perm.as<int32_t>(), pts, conn4, values, cnodes, cperm, C, out,
                                 cell_ids, ctx->d_status, st),
              "sample tets");
+    return GVC_OK;
+}
+
+int gvc_sample_cells(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, const uint8_t* cell_types,
+                     const int64_t* cell_offsets, const int32_t* conn, const double* values, int64_t N,
+                     const float* samples, double* out, int64_t* cell_ids, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (npts < 0 || C < 0 || N < 0) return fail(ctx, GVC_ERR_ARG, "negative size");
+    if (C > kMaxElems || N > kMaxElems) return fail(ctx, GVC_ERR_CAPACITY, "mesh or sample count out of range");
+    if (N > 0 && (!samples || !out)) return fail(ctx, GVC_ERR_ARG, "null pointer");
+    if (C > 0 && (!pts || !cell_types || !cell_offsets || !conn || !values))
+        return fail(ctx, GVC_ERR_ARG, "null mesh pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch* sc = scratch_of(ctx);
+    if (N == 0) return GVC_OK;
+    const int32_t* cperm = nullptr;
+    const BvhNode* cnodes = nullptr;
+    if (C > 0) {
+        GVC_CUDA(sc->tmp_boxes.ensure(sizeof(float4) * 2 * C), "alloc cell boxes");
+        GVC_CUDA(launch_cell_boxes(C, pts, cell_types, cell_offsets, conn, sc->tmp_boxes.as<float4>(), st),
+                 "cell boxes");
+        GVC_CUDA(lbvh_build_boxes(ctx->cells, C, sc->tmp_boxes.as<float4>(), st), "cell LBVH");
+        cperm = ctx->cells.perm.as<int32_t>();
+        cnodes = ctx->cells.nodes.as<BvhNode>();
+    }
+    GVC_CUDA(morton_sort_points(sc->msamp, N, samples, st), "sample order");
+    GVC_CUDA(launch_sample_cells(N, samples, sc->msamp.perm.as<int32_t>(), pts, cell_types, cell_offsets, conn,
+                                 values, cnodes, cperm, C, out, cell_ids, ctx->d_status, st),
+             "sample cells");
     return GVC_OK;
 }
 

@@ -503,6 +503,7 @@ __global__ void __launch_bounds__(kBlockRows + 32) k_forward_cta(
         }
         __syncwarp();
         if (COUNT && lane == 0) {
+            atomicMax(&stats[3], (unsigned long long)tc.max_sp);
             atomicAdd(&stats[5], (unsigned long long)tc.leaves);
             atomicAdd(&stats[6], (unsigned long long)tc.nodes);
         }

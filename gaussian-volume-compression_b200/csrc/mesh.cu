@@ -215,7 +215,211 @@ __global__ void __launch_bounds__(128) k_sample_tets(int64_t N, const float* __r
     if (cell_ids) cell_ids[s] = best;
 }
 
+// ---------------------------------------------------------------------------------
+// General explicit cells: VTK_TETRA (10), VTK_HEXAHEDRON (12), VTK_WEDGE (13),
+// VTK_PYRAMID (14) with isoparametric shape functions in VTK node order; the point is
+// mapped to parametric coordinates by Newton's method in double (same expressions, same
+// iteration rule as the oracle); zero-volume cells (1, 3, 5, 9) never contain a point.
+// ---------------------------------------------------------------------------------
+constexpr int kNewtonIters = 20;
+constexpr double kNewtonTol = 1e-13;
+constexpr double kInsideEps = 1e-9;
+
+__device__ __forceinline__ int cell_npts(int type) {
+    return type == 10 ? 4 : (type == 12 ? 8 : (type == 13 ? 6 : (type == 14 ? 5 : 0)));
+}
+
+__device__ int shape_eval(int type, double r, double s, double t, double N[8], double dN[8][3]) {
+    if (type == 12) {
+        const double rm = 1.0 - r, sm = 1.0 - s, tm = 1.0 - t;
+        N[0] = rm * sm * tm; N[1] = r * sm * tm; N[2] = r * s * tm; N[3] = rm * s * tm;
+        N[4] = rm * sm * t;  N[5] = r * sm * t;  N[6] = r * s * t;  N[7] = rm * s * t;
+        dN[0][0] = -(sm * tm); dN[0][1] = -(rm * tm); dN[0][2] = -(rm * sm);
+        dN[1][0] = sm * tm;    dN[1][1] = -(r * tm);  dN[1][2] = -(r * sm);
+        dN[2][0] = s * tm;     dN[2][1] = r * tm;     dN[2][2] = -(r * s);
+        dN[3][0] = -(s * tm);  dN[3][1] = rm * tm;    dN[3][2] = -(rm * s);
+        dN[4][0] = -(sm * t);  dN[4][1] = -(rm * t);  dN[4][2] = rm * sm;
+        dN[5][0] = sm * t;     dN[5][1] = -(r * t);   dN[5][2] = r * sm;
+        dN[6][0] = s * t;      dN[6][1] = r * t;      dN[6][2] = r * s;
+        dN[7][0] = -(s * t);   dN[7][1] = rm * t;     dN[7][2] = rm * s;
+        return 8;
+    }
+    if (type == 13) {
+        const double u = 1.0 - r - s, tm = 1.0 - t;
+        N[0] = u * tm; N[1] = r * tm; N[2] = s * tm; N[3] = u * t; N[4] = r * t; N[5] = s * t;
+        dN[0][0] = -tm; dN[0][1] = -tm; dN[0][2] = -u;
+        dN[1][0] = tm;  dN[1][1] = 0.0; dN[1][2] = -r;
+        dN[2][0] = 0.0; dN[2][1] = tm;  dN[2][2] = -s;
+        dN[3][0] = -t;  dN[3][1] = -t;  dN[3][2] = u;
+        dN[4][0] = t;   dN[4][1] = 0.0; dN[4][2] = r;
+        dN[5][0] = 0.0; dN[5][1] = t;   dN[5][2] = s;
+        return 6;
+    }
+    if (type == 14) {
+        const double rm = 1.0 - r, sm = 1.0 - s, tm = 1.0 - t;
+        N[0] = rm * sm * tm; N[1] = r * sm * tm; N[2] = r * s * tm; N[3] = rm * s * tm; N[4] = t;
+        dN[0][0] = -(sm * tm); dN[0][1] = -(rm * tm); dN[0][2] = -(rm * sm);
+        dN[1][0] = sm * tm;    dN[1][1] = -(r * tm);  dN[1][2] = -(r * sm);
+        dN[2][0] = s * tm;     dN[2][1] = r * tm;     dN[2][2] = -(r * s);
+        dN[3][0] = -(s * tm);  dN[3][1] = rm * tm;    dN[3][2] = -(rm * s);
+        dN[4][0] = 0.0;        dN[4][1] = 0.0;        dN[4][2] = 1.0;
+        return 5;
+    }
+    return 0;
+}
+
+__device__ int iso_contains(int type, const float* __restrict__ pts, const int32_t* __restrict__ cv, const float* p,
+                            double Nout[8]) {
+    double r, s, t;
+    if (type == 12) { r = 0.5; s = 0.5; t = 0.5; }
+    else if (type == 13) { r = 1.0 / 3.0; s = 1.0 / 3.0; t = 0.5; }
+    else { r = 0.5; s = 0.5; t = 0.25; }
+    double N[8], dN[8][3];
+    int n = 0;
+    bool converged = false;
+    for (int it = 0; it < kNewtonIters; it++) {
+        n = shape_eval(type, r, s, t, N, dN);
+        double f[3] = {0.0, 0.0, 0.0}, J[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+        for (int k = 0; k < n; k++) {
+            const float* x = pts + 3 * (int64_t)cv[k];
+            for (int a = 0; a < 3; a++) {
+                f[a] = f[a] + N[k] * (double)x[a];
+                for (int b = 0; b < 3; b++) J[a][b] = J[a][b] + dN[k][b] * (double)x[a];
+            }
+        }
+        for (int a = 0; a < 3; a++) f[a] = f[a] - (double)p[a];
+        const double det = det3(J[0][0], J[0][1], J[0][2], J[1][0], J[1][1], J[1][2], J[2][0], J[2][1], J[2][2]);
+        if (det == 0.0 || det != det) return 0;
+        const double d0 = det3(f[0], J[0][1], J[0][2], f[1], J[1][1], J[1][2], f[2], J[2][1], J[2][2]) / det;
+        const double d1 = det3(J[0][0], f[0], J[0][2], J[1][0], f[1], J[1][2], J[2][0], f[2], J[2][2]) / det;
+        const double d2 = det3(J[0][0], J[0][1], f[0], J[1][0], J[1][1], f[1], J[2][0], J[2][1], f[2]) / det;
+        r = r - d0;
+        s = s - d1;
+        t = t - d2;
+        double m = fabs(d0);
+        if (fabs(d1) > m) m = fabs(d1);
+        if (fabs(d2) > m) m = fabs(d2);
+        if (!(m >= kNewtonTol)) {
+            converged = true;
+            break;
+        }
+    }
+    // an unconverged iterate says nothing about the point: not contained
+    if (!converged) return 0;
+    const double e = kInsideEps;
+    bool inside;
+    if (type == 13) inside = r >= -e && s >= -e && r + s <= 1.0 + e && t >= -e && t <= 1.0 + e;
+    else inside = r >= -e && r <= 1.0 + e && s >= -e && s <= 1.0 + e && t >= -e && t <= 1.0 + e;
+    if (!inside) return 0;
+    n = shape_eval(type, r, s, t, N, dN);
+    for (int k = 0; k < n; k++) Nout[k] = N[k];
+    return n;
+}
+
+__global__ void __launch_bounds__(256) k_cell_boxes(int64_t C, const float* __restrict__ pts,
+                                                    const uint8_t* __restrict__ types,
+                                                    const int64_t* __restrict__ offsets,
+                                                    const int32_t* __restrict__ conn, float4* __restrict__ boxes) {
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const int n = cell_npts(types[c]);
+    for (int k = 0; k < n; k++) {
+        const float* v = pts + 3 * (int64_t)conn[offsets[c] + k];
+        for (int a = 0; a < 3; a++) {
+            lo[a] = fminf(lo[a], v[a]);
+            hi[a] = fmaxf(hi[a], v[a]);
+        }
+    }
+    boxes[2 * c] = make_float4(lo[0], lo[1], lo[2], 0.f);
+    boxes[2 * c + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
+}
+
+__global__ void __launch_bounds__(128) k_sample_cells(int64_t N, const float* __restrict__ samples,
+                                                      const int32_t* __restrict__ sperm, const float* __restrict__ pts,
+                                                      const uint8_t* __restrict__ types,
+                                                      const int64_t* __restrict__ offsets,
+                                                      const int32_t* __restrict__ conn,
+                                                      const double* __restrict__ values,
+                                                      const BvhNode* __restrict__ nodes,
+                                                      const int32_t* __restrict__ cperm, int64_t C,
+                                                      double* __restrict__ out, int64_t* __restrict__ cell_ids,
+                                                      int* status) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int64_t s = sperm ? sperm[i] : i;
+    const float p[3] = {samples[3 * s], samples[3 * s + 1], samples[3 * s + 2]};
+    int64_t best = -1;
+    double best_v = -1.0;
+    if (C > 0) {
+        int stack[kPointStack];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const int node = stack[--sp];
+            const float4* np = reinterpret_cast<const float4*>(nodes + node);
+            const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), d = __ldg(np + 3);
+            const uint32_t ch[2] = {__float_as_uint(a.w), __float_as_uint(b.w)};
+            const bool hit[2] = {a.x <= p[0] && p[0] <= b.x && a.y <= p[1] && p[1] <= b.y && a.z <= p[2] && p[2] <= b.z,
+                                 c.x <= p[0] && p[0] <= d.x && c.y <= p[1] && p[1] <= d.y && c.z <= p[2] && p[2] <= d.z};
+            for (int k = 0; k < 2; k++) {
+                if (!hit[k]) continue;
+                if (ch[k] & kLeafBit) {
+                    const int64_t cell = cperm[ch[k] & ~kLeafBit];
+                    if (best >= 0 && cell > best) continue;
+                    const int type = types[cell];
+                    const int32_t* cv = conn + offsets[cell];
+                    if (type == 10) {
+                        double lam[4];
+                        if (tet_contains(pts + 3 * (int64_t)cv[0], pts + 3 * (int64_t)cv[1],
+                                         pts + 3 * (int64_t)cv[2], pts + 3 * (int64_t)cv[3], p, lam)) {
+                            double v = lam[0] * values[cv[0]];
+                            v = v + lam[1] * values[cv[1]];
+                            v = v + lam[2] * values[cv[2]];
+                            v = v + lam[3] * values[cv[3]];
+                            best = cell;
+                            best_v = v;
+                        }
+                    } else if (type == 12 || type == 13 || type == 14) {
+                        double Nf[8];
+                        const int n = iso_contains(type, pts, cv, p, Nf);
+                        if (n) {
+                            double v = Nf[0] * values[cv[0]];
+                            for (int q = 1; q < n; q++) v = v + Nf[q] * values[cv[q]];
+                            best = cell;
+                            best_v = v;
+                        }
+                    }
+                } else if (sp < kPointStack) {
+                    stack[sp++] = (int)ch[k];
+                } else {
+                    atomicOr(status, kStatusStackOverflow);
+                }
+            }
+        }
+    }
+    out[s] = best >= 0 ? best_v : -1.0;
+    if (cell_ids) cell_ids[s] = best;
+}
+
 static inline unsigned nbk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t launch_cell_boxes(int64_t C, const float* pts, const uint8_t* types, const int64_t* offsets,
+                              const int32_t* conn, float4* boxes, cudaStream_t st) {
+    if (C <= 0) return cudaSuccess;
+    k_cell_boxes<<<nbk(C, 256), 256, 0, st>>>(C, pts, types, offsets, conn, boxes); gvc::note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sample_cells(int64_t N, const float* samples, const int32_t* sperm, const float* pts,
+                                const uint8_t* types, const int64_t* offsets, const int32_t* conn,
+                                const double* values, const BvhNode* cnodes, const int32_t* cperm, int64_t C,
+                                double* out, int64_t* cell_ids, int* status, cudaStream_t st) {
+    if (N <= 0) return cudaSuccess;
+    k_sample_cells<<<nbk(N, 128), 128, 0, st>>>(N, samples, sperm, pts, types, offsets, conn, values, cnodes, cperm,
+                                                C, out, cell_ids, status); gvc::note_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t launch_sample_uniform(const int64_t dims[3], const float origin[3], const float spacing[3],
                                   const void* values, int dtype, int64_t N, const float* samples, void* out,

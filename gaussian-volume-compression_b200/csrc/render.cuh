@@ -87,6 +87,12 @@ cudaError_t launch_sample_uniform(const int64_t dims[3], const float origin[3], 
                                   const void* values, int dtype, int64_t N, const float* samples, void* out,
                                   cudaStream_t st);
 cudaError_t launch_tet_boxes(int64_t C, const float* pts, const int32_t* conn4, float4* boxes, cudaStream_t st);
+cudaError_t launch_cell_boxes(int64_t C, const float* pts, const uint8_t* types, const int64_t* offsets,
+                              const int32_t* conn, float4* boxes, cudaStream_t st);
+cudaError_t launch_sample_cells(int64_t N, const float* samples, const int32_t* sperm, const float* pts,
+                                const uint8_t* types, const int64_t* offsets, const int32_t* conn,
+                                const double* values, const BvhNode* cnodes, const int32_t* cperm, int64_t C,
+                                double* out, int64_t* cell_ids, int* status, cudaStream_t st);
 cudaError_t launch_sample_tets(int64_t N, const float* samples, const int32_t* sperm, const float* pts,
                                const int32_t* conn4, const double* values, const BvhNode* cnodes,
                                const int32_t* cperm, int64_t C, double* out, int64_t* cell_ids, int* status,

@@ -83,29 +83,38 @@ def sample_mesh(dims_arr, origin_arr, spacing_arr, val_arr, samp_arr):
     return out
 
 
-def _tets_from_cells(conn, cell_types, cell_offsets):
-    """Validates the cells as sample_mesh.cu:300-336 does and returns [C,4] int32 tets."""
+# points per cell for each VTK type the reference maps (sample_mesh.cu:300-336)
+VTK_NPTS = {1: 1, 3: 2, 5: 3, 9: 4, 10: 4, 12: 8, 13: 6, 14: 5}
+
+
+def _check_cells(conn, cell_types, cell_offsets):
+    """Validates the cells as sample_mesh.cu:300-336 does; returns (conn int32, types uint8,
+    offsets int64).  A cell's point count is the distance to the next offset (the last cell
+    ends at the connectivity size) and must equal its type's node count."""
     conn = np.ascontiguousarray(conn, dtype=np.int64).reshape(-1)
     types = np.ascontiguousarray(cell_types, dtype=np.int64).reshape(-1)
     offs = np.ascontiguousarray(cell_offsets, dtype=np.int64).reshape(-1)
     C = types.size
     if C == 0:
-        return np.zeros((0, 4), dtype=np.int32)
+        return conn.astype(np.int32), types.astype(np.uint8), offs[:0].copy()
     if offs.size < C:
         raise RuntimeError("cell_offsets has fewer entries than cell_types")
     unknown = types[~np.isin(types, list(VTK_KNOWN))]
     if unknown.size:
         raise RuntimeError("Unsupported VTK cell type: " + str(int(unknown[0])))
-    if np.any(types != VTK_TETRA):
-        bad = int(types[types != VTK_TETRA][0])
-        raise RuntimeError("VTK cell type %d is not implemented on the GPU path yet (tetrahedra only)" % bad)
     start = offs[:C]
     end = np.empty(C, dtype=np.int64)
     end[:-1] = offs[1:C]
     end[-1] = conn.size
-    if np.any(end - start != 4):
-        raise RuntimeError("tetrahedral cells must have 4 points")
-    idx = start[:, None] + np.arange(4, dtype=np.int64)[None, :]
+    want = np.vectorize(VTK_NPTS.get, otypes=[np.int64])(types)
+    if np.any(end - start != want) or np.any(start < 0) or np.any(end > conn.size):
+        raise RuntimeError("cell point count does not match its VTK cell type")
+    return conn.astype(np.int32), types.astype(np.uint8), start.copy()
+
+
+def _tets_from_cells(conn, types, offs):
+    """[C,4] int32 vertex ids of an all-tetrahedra mesh (already validated)."""
+    idx = offs[:, None] + np.arange(4, dtype=np.int64)[None, :]
     return conn[idx].astype(np.int32)
 
 
@@ -137,8 +146,43 @@ def sample_meshu_cells(pts_arr, conn4, val_arr, samp_arr):
     return d_out.cpu().numpy(), d_cell.cpu().numpy()
 
 
+def sample_meshu_mixed(pts_arr, conn_arr, cell_types_arr, cell_offsets_arr, val_arr, samp_arr):
+    """Samples an explicit mesh of mixed VTK cells; returns (values f64, lowest containing
+    cell id or -1)."""
+    conn, types, offs = _check_cells(conn_arr, cell_types_arr, cell_offsets_arr)
+    pts = np.ascontiguousarray(pts_arr, dtype=np.float32).reshape(-1, 3)
+    vals = np.ascontiguousarray(val_arr, dtype=np.float64).reshape(-1)
+    samples = np.ascontiguousarray(samp_arr, dtype=np.float32).reshape(-1, 3)
+    n, C = samples.shape[0], types.size
+    out = np.full(n, -1.0, dtype=np.float64)
+    cells = np.full(n, -1, dtype=np.int64)
+    if n == 0:
+        return out, cells
+    if conn.size and (conn.min() < 0 or conn.max() >= pts.shape[0]):
+        raise RuntimeError("connectivity refers to a point outside the point array")
+    if vals.size < pts.shape[0]:
+        raise RuntimeError("values must hold one entry per point")
+    dev, c = _ctx()
+    d_pts = _dev(pts, np.float32)
+    d_conn = _dev(conn if conn.size else np.zeros(1, np.int32), np.int32)
+    d_types = _dev(types if C else np.zeros(1, np.uint8), np.uint8)
+    d_offs = _dev(offs if C else np.zeros(1, np.int64), np.int64)
+    d_vals = _dev(vals if vals.size else np.zeros(1), np.float64)
+    d_samp = _dev(samples, np.float32)
+    d_out = torch.empty(n, dtype=torch.float64, device="cuda:%d" % dev)
+    d_cell = torch.empty(n, dtype=torch.int64, device="cuda:%d" % dev)
+    c.call("gvc_sample_cells", pts.shape[0], _n.ptr(d_pts), C, _n.ptr(d_types), _n.ptr(d_offs), _n.ptr(d_conn),
+           _n.ptr(d_vals), n, _n.ptr(d_samp), _n.ptr(d_out), _n.ptr(d_cell), _stream(dev))
+    c.sync_status(torch.cuda.current_stream(dev).cuda_stream)
+    return d_out.cpu().numpy(), d_cell.cpu().numpy()
+
+
 def sample_meshu(pts_arr, conn_arr, cell_types_arr, cell_offsets_arr, val_arr, samp_arr):
-    """Explicit mesh point field sampled at points; outside every cell -> -1 (float64)."""
-    conn4 = _tets_from_cells(conn_arr, cell_types_arr, cell_offsets_arr)
-    out, _ = sample_meshu_cells(pts_arr, conn4, val_arr, samp_arr)
+    """Explicit mesh point field sampled at points; outside every cell -> -1 (float64).
+    All-tetrahedra meshes take the tetrahedral kernel; mixed meshes the general one."""
+    conn, types, offs = _check_cells(conn_arr, cell_types_arr, cell_offsets_arr)
+    if types.size and np.all(types == VTK_TETRA):
+        out, _ = sample_meshu_cells(pts_arr, _tets_from_cells(conn, types, offs), val_arr, samp_arr)
+        return out
+    out, _ = sample_meshu_mixed(pts_arr, conn_arr, cell_types_arr, cell_offsets_arr, val_arr, samp_arr)
     return out

@@ -88,6 +88,67 @@ def jittered_tet_mesh(n=16, seed=0, jitter=0.2):
     return pts, tets
 
 
+def mixed_cell_mesh(n=6, seed=0, jitter=0.2, kinds=(12, 13, 14, 10), extras=True):
+    """A conforming mixed explicit mesh in VTK layout over an n^3 hex grid on [0,1]^3.
+    Each (i, j) column of hexes is one kind: 12 a hexahedron per grid cell, 13 two wedges
+    split along the cell's (1, 3) diagonal, 14 six pyramids on the cell's faces with the
+    cell centre as apex, 10 the six Kuhn tetrahedra.  Columns keep shared faces conforming
+    (hex, wedge-side and pyramid-base faces are the same bilinear quads; triangles meet
+    triangles).  Tetrahedra split quads into triangles, so with 10 among the kinds the grid
+    is mapped by a random affine map instead of jittered (every quad stays planar).
+    extras appends zero-volume cells (VTK 1, 3, 5, 9) that never contain a point.
+    Returns (pts [V,3] f32, conn int64, types int64 [C], offsets int64 [C+1])."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 / n
+    c = np.arange(n + 1) * h
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    grid = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    if 10 in kinds:
+        A = np.eye(3) + rng.uniform(-0.25, 0.25, (3, 3))
+        grid = grid @ A.T + rng.uniform(-1, 1, 3)
+    else:
+        interior = np.all((grid > 0.5 * h) & (grid < 1 - 0.5 * h), axis=1)
+        grid[interior] += rng.uniform(-jitter, jitter, (interior.sum(), 3)) * h
+    N1 = n + 1
+
+    def vid(i, j, k):
+        return (k * N1 + j) * N1 + i
+
+    centres = []
+    conn, types = [], []
+    col_kind = rng.choice(np.asarray(kinds), size=(n, n))
+    for k in range(n):
+        for j in range(n):
+            for i in range(n):
+                hx = [vid(i, j, k), vid(i + 1, j, k), vid(i + 1, j + 1, k), vid(i, j + 1, k),
+                      vid(i, j, k + 1), vid(i + 1, j, k + 1), vid(i + 1, j + 1, k + 1), vid(i, j + 1, k + 1)]
+                kind = int(col_kind[j, i])
+                if kind == 12:
+                    conn.append(hx); types.append(12)
+                elif kind == 13:
+                    conn.append([hx[0], hx[1], hx[3], hx[4], hx[5], hx[7]]); types.append(13)
+                    conn.append([hx[1], hx[2], hx[3], hx[5], hx[6], hx[7]]); types.append(13)
+                elif kind == 14:
+                    apex = grid.shape[0] + len(centres)
+                    centres.append(grid[hx].mean(axis=0))
+                    for f in ((0, 1, 2, 3), (4, 7, 6, 5), (0, 4, 5, 1), (3, 2, 6, 7), (0, 3, 7, 4), (1, 5, 6, 2)):
+                        conn.append([hx[q] for q in f] + [apex]); types.append(14)
+                else:
+                    lat = [vid(i + (b & 1), j + ((b >> 1) & 1), k + ((b >> 2) & 1)) for b in range(8)]
+                    for a, b in ((1, 2), (1, 4), (2, 1), (2, 4), (4, 1), (4, 2)):
+                        conn.append([lat[0], lat[a], lat[a | b], lat[7]]); types.append(10)
+    pts = np.concatenate([grid, np.asarray(centres).reshape(-1, 3)]) if centres else grid
+    if extras:
+        V = grid.shape[0]
+        for t, m in ((1, 1), (3, 2), (5, 3), (9, 4)):
+            at = int(rng.integers(0, len(conn) + 1))
+            conn.insert(at, [int(q) for q in rng.integers(0, V, m)]); types.insert(at, t)
+    offsets = np.zeros(len(conn) + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum([len(q) for q in conn])
+    flat = np.asarray([q for cc in conn for q in cc], dtype=np.int64)
+    return pts.astype(np.float32), flat, np.asarray(types, dtype=np.int64), offsets
+
+
 def blob_field(pts, seed=0, nblobs=32):
     rng = np.random.default_rng(seed + 7)
     c = rng.random((nblobs, 3))

@@ -45,11 +45,13 @@ typedef enum {
                                    use_gaussian_bvh != 0 -> sample-tile traversal with warp
                                    pre-reduction + FP32 atomics (mirrors backward.cu:339-559);
                                1 = always deterministic, 2 = always atomic                */
-    GVC_OPT_EVAL_PATH = 3,  /* forward evaluation kernel:
-                               0 = plain FP32 exponent, one warp per 32-sample tile (default),
-                               1 = tensor-core exponent: tcgen05 BF16 3-way split MMA into TMEM,
-                                   one CTA per 128-sample block,
-                               2 = plain FP32 exponent with the CTA structure of path 1     */
+    GVC_OPT_EVAL_PATH = 3,  /* forward evaluation kernel (all compute the same field):
+                               0 = FP32 exponent, one CTA per 128-sample block: a producer warp
+                                   walks the Gaussian LBVH and stages batches, four consumer
+                                   warps evaluate (default, fastest),
+                               1 = tensor-core exponent: the same pipeline with the power as a
+                                   tcgen05 BF16 3-way split MMA into TMEM,
+                               2 = FP32 exponent, one warp per 32-sample tile               */
     GVC_OPT_COUNT_PAIRS = 4,/* 1 = record per-call pair counts (gvc_get_stats)            */
     GVC_OPT_TIME_KERNELS = 5 /* 1 = time the evaluation kernels with CUDA events on the
                                 caller's stream (gvc_get_stats)                          */
@@ -132,6 +134,17 @@ int gvc_sample_uniform(gvc_ctx* ctx, const int64_t* dims, const float* origin, c
 int gvc_sample_tets(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, const int32_t* conn4,
                     const double* values, int64_t N, const float* samples, double* out, int64_t* cell_ids,
                     void* stream);
+
+/* Replaces sample_meshu for mixed explicit meshes (gpu_sampling/sample_mesh.cu:242-414,
+   cell types mapped at :300-336).  cell_types [C] uint8 VTK ids: 10 tetra, 12 hexahedron,
+   13 wedge, 14 pyramid are located (isoparametric, Newton inversion in double); 1 vertex,
+   3 line, 5 triangle, 9 quad have no volume and never contain a probe point.
+   cell_offsets [C] int64: first connectivity entry of each cell; conn int32 vertex ids;
+   values [npts] float64.  out [N] float64 (value or -1), cell_ids [N] int64 (lowest
+   containing cell or -1, may be NULL).  All device pointers. */
+int gvc_sample_cells(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, const uint8_t* cell_types,
+                     const int64_t* cell_offsets, const int32_t* conn, const double* values, int64_t N,
+                     const float* samples, double* out, int64_t* cell_ids, void* stream);
 
 /* No counterpart in the reference.  Tetrahedral sampling for callers that cannot
    allocate device memory (their memory belongs to another allocator, or cudaMalloc's

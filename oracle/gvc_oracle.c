@@ -984,3 +984,185 @@ void orc_sample_tets(int64_t npts, const float* pts, int64_t C, const int64_t* c
     grid_free(&g);
     free(boxes);
 }
+
+/* ------------------------------------------------------------------------------------
+ * General explicit cells (gpu_sampling/sample_mesh.cu:300-336 maps VTK types 1,3,5,9,10,
+ * 12,13,14 to Viskores shapes).  Declared semantics:
+ *   10 tetra: as orc_sample_tets;
+ *   12 hexahedron, 13 wedge, 14 pyramid: isoparametric shape functions in VTK node order
+ *      hex:   N = (1-r)(1-s)(1-t), r(1-s)(1-t), rs(1-t), (1-r)s(1-t), (1-r)(1-s)t, r(1-s)t, rst, (1-r)st
+ *      wedge: N = (1-r-s)(1-t), r(1-t), s(1-t), (1-r-s)t, rt, st
+ *      pyram: N = (1-r)(1-s)(1-t), r(1-s)(1-t), rs(1-t), (1-r)s(1-t), t
+ *      the point is mapped to (r,s,t) by Newton's method in double (start at the cell's
+ *      parametric centre, at most 20 iterations, stop when max|dr| < 1e-13, singular
+ *      Jacobian -> outside), inside iff every parametric bound holds within 1e-9
+ *      (hex: 0 <= r,s,t <= 1; wedge: r,s >= 0, r+s <= 1, 0 <= t <= 1; pyramid: 0 <= r,s,t <= 1);
+ *   1 vertex, 3 line, 5 triangle, 9 quad: zero volume, never contain a probe point.
+ *   Ties -> the lowest cell id; outside every cell -> -1.
+ * The same expressions (no FMA contraction) run on the GPU.
+ * ------------------------------------------------------------------------------------ */
+#define ORC_NEWTON_ITERS 20
+#define ORC_NEWTON_TOL 1e-13
+#define ORC_INSIDE_EPS 1e-9
+
+static int shape_eval(int type, double r, double s, double t, double N[8], double dN[8][3]) {
+    switch (type) {
+        case 12: {
+            double rm = 1.0 - r, sm = 1.0 - s, tm = 1.0 - t;
+            N[0] = rm * sm * tm; N[1] = r * sm * tm; N[2] = r * s * tm; N[3] = rm * s * tm;
+            N[4] = rm * sm * t;  N[5] = r * sm * t;  N[6] = r * s * t;  N[7] = rm * s * t;
+            dN[0][0] = -(sm * tm); dN[0][1] = -(rm * tm); dN[0][2] = -(rm * sm);
+            dN[1][0] = sm * tm;    dN[1][1] = -(r * tm);  dN[1][2] = -(r * sm);
+            dN[2][0] = s * tm;     dN[2][1] = r * tm;     dN[2][2] = -(r * s);
+            dN[3][0] = -(s * tm);  dN[3][1] = rm * tm;    dN[3][2] = -(rm * s);
+            dN[4][0] = -(sm * t);  dN[4][1] = -(rm * t);  dN[4][2] = rm * sm;
+            dN[5][0] = sm * t;     dN[5][1] = -(r * t);   dN[5][2] = r * sm;
+            dN[6][0] = s * t;      dN[6][1] = r * t;      dN[6][2] = r * s;
+            dN[7][0] = -(s * t);   dN[7][1] = rm * t;     dN[7][2] = rm * s;
+            return 8;
+        }
+        case 13: {
+            double u = 1.0 - r - s, tm = 1.0 - t;
+            N[0] = u * tm; N[1] = r * tm; N[2] = s * tm; N[3] = u * t; N[4] = r * t; N[5] = s * t;
+            dN[0][0] = -tm; dN[0][1] = -tm; dN[0][2] = -u;
+            dN[1][0] = tm;  dN[1][1] = 0.0; dN[1][2] = -r;
+            dN[2][0] = 0.0; dN[2][1] = tm;  dN[2][2] = -s;
+            dN[3][0] = -t;  dN[3][1] = -t;  dN[3][2] = u;
+            dN[4][0] = t;   dN[4][1] = 0.0; dN[4][2] = r;
+            dN[5][0] = 0.0; dN[5][1] = t;   dN[5][2] = s;
+            return 6;
+        }
+        case 14: {
+            double rm = 1.0 - r, sm = 1.0 - s, tm = 1.0 - t;
+            N[0] = rm * sm * tm; N[1] = r * sm * tm; N[2] = r * s * tm; N[3] = rm * s * tm; N[4] = t;
+            dN[0][0] = -(sm * tm); dN[0][1] = -(rm * tm); dN[0][2] = -(rm * sm);
+            dN[1][0] = sm * tm;    dN[1][1] = -(r * tm);  dN[1][2] = -(r * sm);
+            dN[2][0] = s * tm;     dN[2][1] = r * tm;     dN[2][2] = -(r * s);
+            dN[3][0] = -(s * tm);  dN[3][1] = rm * tm;    dN[3][2] = -(rm * s);
+            dN[4][0] = 0.0;        dN[4][1] = 0.0;        dN[4][2] = 1.0;
+            return 5;
+        }
+    }
+    return 0;
+}
+
+/* Newton inversion + inside test; on success writes the shape function values. */
+static int iso_contains(int type, const float* pts, const int32_t* cv, const float* p, double Nout[8]) {
+    double r, s, t;
+    if (type == 12) { r = 0.5; s = 0.5; t = 0.5; }
+    else if (type == 13) { r = 1.0 / 3.0; s = 1.0 / 3.0; t = 0.5; }
+    else { r = 0.5; s = 0.5; t = 0.25; }
+    double N[8], dN[8][3];
+    int n = 0, converged = 0;
+    for (int it = 0; it < ORC_NEWTON_ITERS; it++) {
+        n = shape_eval(type, r, s, t, N, dN);
+        double f[3] = {0.0, 0.0, 0.0}, J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int k = 0; k < n; k++) {
+            const float* x = pts + 3 * (int64_t)cv[k];
+            for (int a = 0; a < 3; a++) {
+                f[a] = f[a] + N[k] * (double)x[a];
+                for (int b = 0; b < 3; b++) J[a][b] = J[a][b] + dN[k][b] * (double)x[a];
+            }
+        }
+        for (int a = 0; a < 3; a++) f[a] = f[a] - (double)p[a];
+        double det = det3(J[0][0], J[0][1], J[0][2], J[1][0], J[1][1], J[1][2], J[2][0], J[2][1], J[2][2]);
+        if (det == 0.0 || det != det) return 0;
+        /* Cramer's rule for J d = f */
+        double d0 = det3(f[0], J[0][1], J[0][2], f[1], J[1][1], J[1][2], f[2], J[2][1], J[2][2]) / det;
+        double d1 = det3(J[0][0], f[0], J[0][2], J[1][0], f[1], J[1][2], J[2][0], f[2], J[2][2]) / det;
+        double d2 = det3(J[0][0], J[0][1], f[0], J[1][0], J[1][1], f[1], J[2][0], J[2][1], f[2]) / det;
+        r = r - d0;
+        s = s - d1;
+        t = t - d2;
+        double m = fabs(d0);
+        if (fabs(d1) > m) m = fabs(d1);
+        if (fabs(d2) > m) m = fabs(d2);
+        if (!(m >= ORC_NEWTON_TOL)) {
+            converged = 1;
+            break;
+        }
+    }
+    /* an unconverged iterate says nothing about the point: not contained */
+    if (!converged) return 0;
+    const double e = ORC_INSIDE_EPS;
+    int inside;
+    if (type == 13) inside = r >= -e && s >= -e && r + s <= 1.0 + e && t >= -e && t <= 1.0 + e;
+    else inside = r >= -e && r <= 1.0 + e && s >= -e && s <= 1.0 + e && t >= -e && t <= 1.0 + e;
+    if (!inside) return 0;
+    n = shape_eval(type, r, s, t, N, dN);
+    for (int k = 0; k < n; k++) Nout[k] = N[k];
+    return n;
+}
+
+static int cell_npts(int type) {
+    switch (type) {
+        case 10: return 4;
+        case 12: return 8;
+        case 13: return 6;
+        case 14: return 5;
+    }
+    return 0;
+}
+
+/* types[C] (VTK ids), offsets[C] (start of each cell in conn), conn int32. */
+void orc_sample_cells(int64_t npts, const float* pts, int64_t C, const uint8_t* types, const int64_t* offsets,
+                      const int32_t* conn, const double* values, int64_t N, const float* samples, double* out,
+                      int64_t* cell, int nthreads) {
+    int nt = orc_nthreads(nthreads);
+    (void)npts;
+    float* boxes = (float*)malloc(sizeof(float) * 6 * (size_t)(C ? C : 1));
+    for (int64_t c = 0; c < C; c++) {
+        int n = cell_npts(types[c]);
+        for (int a = 0; a < 3; a++) { boxes[6 * c + a] = INFINITY; boxes[6 * c + 3 + a] = -INFINITY; }
+        for (int k = 0; k < n; k++) {
+            const float* v = pts + 3 * (int64_t)conn[offsets[c] + k];
+            for (int a = 0; a < 3; a++) {
+                boxes[6 * c + a] = fminf(boxes[6 * c + a], v[a]);
+                boxes[6 * c + 3 + a] = fmaxf(boxes[6 * c + 3 + a], v[a]);
+            }
+        }
+    }
+    double glo[3], ghi[3];
+    boxes_bounds(C, boxes, glo, ghi);
+    orc_grid g;
+    grid_build(&g, C, boxes, glo, ghi, median_extent(C, boxes), nt);
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1024)
+    for (int64_t s = 0; s < N; s++) {
+        const float* p = samples + 3 * s;
+        out[s] = -1.0;
+        cell[s] = -1;
+        if (C == 0) continue;
+        int64_t cl = grid_cell_of_point(&g, p);
+        if (cl < 0) continue;
+        for (int64_t k = g.start[cl]; k < g.start[cl + 1]; k++) {
+            int32_t c = g.items[k];
+            if (!in_box(boxes + 6 * (int64_t)c, p[0], p[1], p[2])) continue;
+            const int32_t* cv = conn + offsets[c];
+            int type = types[c];
+            if (type == 10) {
+                double lam[4];
+                if (tet_contains(pts + 3 * cv[0], pts + 3 * cv[1], pts + 3 * cv[2], pts + 3 * cv[3], p, lam)) {
+                    double v = lam[0] * values[cv[0]];
+                    v = v + lam[1] * values[cv[1]];
+                    v = v + lam[2] * values[cv[2]];
+                    v = v + lam[3] * values[cv[3]];
+                    out[s] = v;
+                    cell[s] = c;
+                    break;
+                }
+            } else if (type == 12 || type == 13 || type == 14) {
+                double Nf[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                int n = iso_contains(type, pts, cv, p, Nf);
+                if (n) {
+                    double v = Nf[0] * values[cv[0]];
+                    for (int q = 1; q < n; q++) v = v + Nf[q] * values[cv[q]];
+                    out[s] = v;
+                    cell[s] = c;
+                    break;
+                }
+            }
+        }
+    }
+    grid_free(&g);
+    free(boxes);
+}

@@ -58,6 +58,7 @@ def lib():
             "orc_sample_uniform": [vp, vp, vp, vp, i64, vp, vp, vp, i32],
             "orc_sample_tets": [i64, vp, i64, vp, vp, i64, vp, vp, vp, i32],
             "orc_tet_boxes": [i64, vp, vp, vp],
+            "orc_sample_cells": [i64, vp, i64, vp, vp, vp, vp, i64, vp, vp, vp, i32],
             "orc_openmp_enabled": [],
         }
         for name, args in sig.items():
@@ -220,6 +221,22 @@ def sample_tets(pts, conn4, values, samples, nthreads=0):
     return out, cell
 
 
+def sample_cells(pts, types, offsets, conn, values, samples, nthreads=0):
+    """Mixed explicit cells (VTK 10/12/13/14 located, 1/3/5/9 never contain a point);
+    returns (values f64 or -1, lowest containing cell id or -1)."""
+    pts = _c(pts, np.float32).reshape(-1, 3)
+    types = _c(types, np.uint8).reshape(-1)
+    offsets = _c(offsets, np.int64).reshape(-1)
+    conn = _c(conn, np.int32).reshape(-1)
+    values = _c(values, np.float64).reshape(-1)
+    samples = _c(samples, np.float32).reshape(-1, 3)
+    n = samples.shape[0]
+    out = np.zeros(n); cell = np.zeros(n, np.int64)
+    lib().orc_sample_cells(pts.shape[0], _p(pts), types.shape[0], _p(types), _p(offsets), _p(conn), _p(values), n,
+                           _p(samples), _p(out), _p(cell), nthreads)
+    return out, cell
+
+
 # --------------------------------------------------------------------------------------
 # Reference Python layers (FP64 restatements)
 # --------------------------------------------------------------------------------------
@@ -300,4 +317,4 @@ _PKG = os.path.join(os.path.dirname(HERE), "gaussian-volume-compression_b200")
 if _PKG not in _sys.path:
     _sys.path.insert(0, _PKG)
 from gvc_workloads import (mixture_small, grid_centres, blob_target, mixture_large,  # noqa: E402,F401
-                           jittered_tet_mesh, blob_field)
+                           jittered_tet_mesh, mixed_cell_mesh, blob_field)

@@ -64,6 +64,8 @@ def test_mesh_sampler_argument_errors():
     pts = np.random.rand(8, 3).astype(np.float32)
     with pytest.raises(RuntimeError, match="Unsupported VTK cell type: 42"):
         gpu_sampleu(pts, np.arange(4), np.array([42]), np.array([0]), np.zeros(8), np.zeros((1, 3)))
+    with pytest.raises(RuntimeError, match="does not match its VTK cell type"):
+        gpu_sampleu(pts, np.arange(5), np.array([12]), np.array([0]), np.zeros(8), np.zeros((1, 3)))
 
 
 def test_mesh_sampler_output_dtypes_without_samples():

@@ -58,3 +58,32 @@ def test_sampleu_vtk_arrays(cuda, orc):
     ref, _ = orc.sample_tets(pts, tets, vals, q)
     assert out.dtype == np.float64
     np.testing.assert_array_equal(out, ref)
+
+
+@pytest.mark.parametrize("kinds,n,ns", [((12,), 6, 50000), ((13,), 6, 50000), ((14,), 6, 50000),
+                                        ((12, 13, 14), 16, 400000), ((12, 13, 14, 10), 12, 200000)])
+def test_mixed_cells_bit_exact(cuda, orc, kinds, n, ns):
+    from gpu_mesh_sampling._gpu_mesh_sampling import sample_meshu_mixed
+    pts, conn, types, offs = orc.mixed_cell_mesh(n=n, seed=n, kinds=kinds)
+    vals = orc.blob_field(pts).astype(np.float64)
+    rng = np.random.default_rng(n)
+    lo, hi = pts.min(0), pts.max(0)
+    q = (lo - 0.01 + rng.random((ns, 3)) * (hi - lo + 0.02)).astype(np.float32)
+    q[:1000] = pts[conn[rng.integers(0, conn.size, 1000)]]       # on vertices shared by several cells
+    out, cell = sample_meshu_mixed(pts, conn, types, offs, vals, q)
+    ref, rcell = orc.sample_cells(pts, types, offs[:-1], conn, vals, q)
+    np.testing.assert_array_equal(cell, rcell)
+    np.testing.assert_array_equal(out, ref)
+    # the affinely mapped grid (with tetrahedra) fills about half of its bounding box
+    assert (cell >= 0).mean() > (0.3 if 10 in kinds else 0.5)
+
+
+def test_sampleu_mixed_vtk_arrays(cuda, orc):
+    from gpu_mesh_sampling import gpu_sampleu
+    pts, conn, types, offs = orc.mixed_cell_mesh(n=8, seed=4, kinds=(12, 13, 14))
+    vals = orc.blob_field(pts).astype(np.float64)
+    q = np.random.default_rng(3).random((20000, 3)).astype(np.float32)
+    out = gpu_sampleu(pts, conn, types, offs, vals, q)
+    ref, _ = orc.sample_cells(pts, types, offs[:-1], conn, vals, q)
+    assert out.dtype == np.float64
+    np.testing.assert_array_equal(out, ref)

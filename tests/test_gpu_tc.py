@@ -1,5 +1,6 @@
-"""Tensor-core (tcgen05) path: the MMA building block through the C ABI, and the CTA
-forward with the tensor-core exponent (and its FP32 SIMT twin) against the oracle.
+"""Tensor-core (tcgen05) path: the MMA building block through the C ABI, and the forward with
+the tensor-core exponent (and the warp-per-tile FP32 kernel) against the oracle; the
+default FP32 CTA forward is covered by test_gpu_rasterizer.py.
 
 Tolerances: the GEMM hook is exact on small integers and within 1e-6 (relative to the
 row norm) on random BF16 data; the plain CTA forward meets the plain tolerance (2e-5);
@@ -67,7 +68,7 @@ def case(cuda, orc):
     return means, scales, rots, values, weights, orc.grid_centres(64)
 
 
-@pytest.mark.parametrize("path,tol", [("plain_cta", 2e-5), ("tensor_core", 1e-4)])
+@pytest.mark.parametrize("path,tol", [("plain_tile", 2e-5), ("tensor_core", 1e-4)])
 def test_cta_forward_matches_oracle(cuda, orc, case, path, tol):
     means, scales, rots, values, weights, samples = case
     out, outw, conics = run_path(cuda, case, path)
@@ -89,7 +90,7 @@ def test_tensor_core_forward_large_clustered(cuda, orc):
     case = (means, scales, rots, values, weights, samples)
     a = [x.cpu().numpy() for x in run_path(cuda, case, "plain")[:2]]
     b = [x.cpu().numpy() for x in run_path(cuda, case, "tensor_core")[:2]]
-    c = [x.cpu().numpy() for x in run_path(cuda, case, "plain_cta")[:2]]
+    c = [x.cpu().numpy() for x in run_path(cuda, case, "plain_tile")[:2]]
     for other, tol in ((c, 2e-5), (b, 1e-4)):
         near = np.abs(a[1] - 0.01) <= 1e-6 + 4e-6
         ok = ~near

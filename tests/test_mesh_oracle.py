@@ -58,3 +58,67 @@ def test_tet_grid_search_matches_brute_force(orc):
                 best = c
                 break
         assert best == cell[s]
+
+
+def _unit_cube_points(pts, n, q01):
+    """Maps points of [0,1]^3 into the (affinely mapped) grid of mixed_cell_mesh."""
+    N1 = n + 1
+    g0 = pts[0].astype(np.float64)
+    e = np.stack([pts[n], pts[n * N1], pts[n * N1 * N1]]).astype(np.float64) - g0
+    return (g0 + q01 @ e).astype(np.float32)
+
+
+def _linear(pts, a=(0.3, -1.2, 2.0), b=0.7):
+    return pts.astype(np.float64) @ np.asarray(a) + b
+
+
+def test_cells_reproduce_linear_field(orc):
+    """Every isoparametric cell reproduces a linear field (partition of unity) and the
+    conforming mixed mesh leaves no gaps."""
+    rng = np.random.default_rng(5)
+    for kinds in ((12,), (13,), (14,), (12, 13, 14), (12, 13, 14, 10)):
+        n = 5
+        pts, conn, types, offs = orc.mixed_cell_mesh(n=n, seed=len(kinds), kinds=kinds)
+        q01 = 0.01 + 0.98 * rng.random((8000, 3))
+        q = _unit_cube_points(pts, n, q01) if 10 in kinds else q01.astype(np.float32)
+        out, cell = orc.sample_cells(pts, types, offs[:-1], conn, _linear(pts), q)
+        assert (cell >= 0).all(), kinds
+        assert set(np.unique(types[cell])) <= set(kinds)
+        np.testing.assert_allclose(out, _linear(q), rtol=0, atol=1e-9)
+        far = np.array([[2.0, 2.0, 2.0], [-1.0, 0.5, 0.5]], np.float32)
+        out2, cell2 = orc.sample_cells(pts, types, offs[:-1], conn, _linear(pts), far)
+        assert (cell2 == -1).all() and (out2 == -1.0).all()
+
+
+def test_cells_trilinear_hex_and_lowest_id(orc):
+    """A single-hex field that is trilinear in the hex's own parameters comes back exactly
+    at mapped points; a vertex shared by several cells resolves to the lowest cell id."""
+    pts, conn, types, offs = orc.mixed_cell_mesh(n=3, seed=7, kinds=(12,), jitter=0.0, extras=False)
+    f = lambda p: 1.0 + p[:, 0] - 2 * p[:, 1] + 0.5 * p[:, 2] + 3 * p[:, 0] * p[:, 1] * p[:, 2]
+    vals = f(pts.astype(np.float64))
+    q = (np.random.default_rng(0).random((2000, 3))).astype(np.float32)
+    out, cell = orc.sample_cells(pts, types, offs[:-1], conn, vals, q)
+    assert (cell >= 0).all()
+    np.testing.assert_allclose(out, f(q.astype(np.float64)), rtol=0, atol=1e-9)
+    v = np.array([[1 / 3, 1 / 3, 1 / 3]], np.float32)          # grid vertex shared by 8 hexes
+    _, c = orc.sample_cells(pts, types, offs[:-1], conn, vals, v)
+    owners = [k for k in range(types.size)
+              if (np.abs(pts[conn[offs[k]:offs[k + 1]]] - v).sum(1) < 1e-7).any()]
+    assert c[0] == min(owners)
+
+
+def test_cells_zero_volume_types_and_tet_agreement(orc):
+    """VTK vertex/line/triangle/quad cells never contain a point; an all-tet mesh gives the
+    tetrahedral sampler's answer bit for bit."""
+    pts, tets = orc.jittered_tet_mesh(n=4, seed=3)
+    vals = orc.blob_field(pts).astype(np.float64)
+    q = np.random.default_rng(1).random((3000, 3)).astype(np.float32)
+    C = tets.shape[0]
+    ref, rcell = orc.sample_tets(pts, tets, vals, q)
+    out, cell = orc.sample_cells(pts, np.full(C, 10), np.arange(C) * 4, tets.reshape(-1), vals, q)
+    np.testing.assert_array_equal(cell, rcell)
+    np.testing.assert_array_equal(out, ref)
+    conn = np.array([0, 1, 2, 0, 1, 5, 7, 9, 11], np.int32)
+    types = np.array([1, 3, 5], np.uint8)
+    out, cell = orc.sample_cells(pts, types, np.array([0, 1, 3]), conn, vals, pts[:50])
+    assert (cell == -1).all() and (out == -1.0).all()
