@@ -325,7 +325,8 @@ def run_ours(args):
                           "fwd_tile_gaussian_evals": counts["fwd_leaf_hits"],
                           "fwd_node_visits": counts["fwd_node_visits"],
                           "bwd_leaf_evals": counts["bwd_leaf_hits"],
-                          "bwd_node_visits": counts["bwd_node_visits"]},
+                          "bwd_node_visits": counts["bwd_node_visits"],
+                          "fwd_lane_evals": counts["fwd_lane_evals"], "bwd_rows": counts["bwd_rows"]},
                 "flops_per_pair": {"candidate": F_CAND, "fwd_contributing": F_FWD_CONTRIB,
                                    "bwd_contributing": F_BWD_CONTRIB, "ex2_fp32_equiv": EX2_EQUIV}}
 

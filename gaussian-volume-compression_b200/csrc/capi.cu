@@ -185,7 +185,7 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
                           &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds};
         for (DevBuf* b : bufs) b->release();
     }
-    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->s_grad, &c->grec, &c->gtmp,
+    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
                       &c->m_out_sorted, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
     for (DevBuf* b : bufs) b->release();
     if (c->d_status) cudaFree(c->d_status);
@@ -243,6 +243,8 @@ int gvc_get_stats(gvc_ctx* ctx, gvc_stats* out, void* stream) {
     out->fwd_node_visits = (int64_t)h[6];
     out->bwd_leaf_hits = (int64_t)h[7];
     out->bwd_node_visits = (int64_t)h[8];
+    out->fwd_lane_evals = (int64_t)h[9];
+    out->bwd_rows = (int64_t)h[10];
     drain_events(ctx);
     out->fwd_kernel_ms = ctx->fwd_kernel_ms;
     out->bwd_kernel_ms = ctx->bwd_kernel_ms;
@@ -413,8 +415,11 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
     } else {
         const int64_t slots = ctx->n_tiles * kTile;
         GVC_CUDA(ctx->s_grad.ensure(sizeof(float4) * slots), "alloc s_grad");
+        GVC_CUDA(ctx->s_gyz.ensure(sizeof(float) * slots), "alloc s_gyz");
+        GVC_CUDA(ctx->s_ok.ensure(slots), "alloc s_ok");
         GVC_CUDA(launch_sample_grads(slots, ctx->s_sorted.as<float4>(), out_cells, out_weights, dL_dout_cells,
-                                     dL_dout_weights, ctx->s_grad.as<float4>(), st),
+                                     dL_dout_weights, ctx->s_grad.as<float4>(), ctx->s_gyz.as<float>(),
+                                     ctx->s_ok.as<uint8_t>(), st),
                  "sample grads");
         BwdArgs ba;
         ba.P = P;
@@ -425,6 +430,8 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
         ba.boxes = boxes;
         ba.s_sorted = ctx->s_sorted.as<float4>();
         ba.s_grad = ctx->s_grad.as<float4>();
+        ba.s_gyz = ctx->s_gyz.as<float>();
+        ba.s_ok = ctx->s_ok.as<uint8_t>();
         ba.tile_boxes = ctx->tile_boxes.as<float4>();
         ba.gdesc = ctx->tile_gdesc.as<uint32_t>();
         ba.n_tiles = ctx->n_tiles;

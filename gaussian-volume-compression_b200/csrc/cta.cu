@@ -246,12 +246,22 @@ __device__ __forceinline__ bool overlap6(const Box6& b, float4 lo, float4 hi) {
     return lo.x <= b.hx && hi.x >= b.lx && lo.y <= b.hy && hi.y >= b.ly && lo.z <= b.hz && hi.z >= b.lz;
 }
 
-struct CtaSmem {
-    unsigned char A[3][kBlockRows * 32];           // phi(u), three bf16 parts
-    unsigned char B[kStages][3][kBatch * 32];      // beta, three bf16 parts, per stage
+// Tensor-core operands (first in the block, 1024-byte aligned); absent in the SIMT variant,
+// whose smaller footprint lets more CTAs share an SM.
+template <bool TC>
+struct CtaTcOperands {
+    unsigned char A[3][kBlockRows * 32];       // phi(u), three bf16 parts
+    unsigned char B[kStages][3][kBatch * 32];  // beta, three bf16 parts, per stage
+};
+template <>
+struct CtaTcOperands<false> {};
+
+template <bool TC>
+struct CtaSmem : CtaTcOperands<TC> {
     float4 gd[kStages][kBatch][5];                 // (mu, w), C'(0..3), (C'4, C'5, v, -), lo, hi
     uint8_t colmask[kStages][kBatch];              // bits 0..3: column overlaps warp w; bit 4: SIMT fallback
     int2 desc[kStages];                            // (number of columns or -1 at the end, group)
+    Box6 wb[4];                                    // boxes of the current group's rows of each consumer warp
     int stack[kStackCap];
     int cand[kCandCap];
     uint64_t full[kStages], empty[kStages];
@@ -273,7 +283,7 @@ __device__ __forceinline__ void cp_async_wait() {
 // the next batch's copies are in flight.
 template <bool TC, bool COUNT>
 struct Producer {
-    CtaSmem& sm;
+    CtaSmem<TC>& sm;
     const GaussRec* __restrict__ recs;
     int* status;
     uint32_t tmem;
@@ -282,7 +292,6 @@ struct Producer {
     int pend_stage, pend_nb;
     int g;
     float x0, y0, z0, ex, ey, ez;
-    Box6 wb[4];
     bool failed;
 
     // waits until the consumers have released the previous use of the stage of batch n
@@ -304,8 +313,8 @@ struct Producer {
             sm.gd[s][lane][1] = make_float4(c0, 2.f * c1, 2.f * c2, c3);
             sm.gd[s][lane][2] = make_float4(2.f * c4, c5, r2.z, 0.f);
 #pragma unroll
-            for (int ww = 0; ww < 4; ww++) cm |= overlap6(wb[ww], r3, r4) ? (uint8_t)(1u << ww) : (uint8_t)0;
-            if (TC) {
+            for (int ww = 0; ww < 4; ww++) cm |= overlap6(sm.wb[ww], r3, r4) ? (uint8_t)(1u << ww) : (uint8_t)0;
+            if constexpr (TC) {
                 const float mx = r0.x - x0, my = r0.y - y0, mz = r0.z - z0;
                 const float cmx = c0 * mx + c1 * my + c2 * mz;
                 const float cmy = c1 * mx + c3 * my + c4 * mz;
@@ -333,7 +342,7 @@ struct Producer {
                 store_row_k16(sm.B[s][1], lane, m);
                 store_row_k16(sm.B[s][2], lane, l);
             }
-        } else if (TC) {
+        } else if constexpr (TC) {
             __nv_bfloat16 zz[16];
 #pragma unroll
             for (int q = 0; q < 16; q++) zz[q] = __float2bfloat16_rn(0.f);
@@ -346,7 +355,7 @@ struct Producer {
         if (TC) fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) {
-            if (TC) {
+            if constexpr (TC) {
                 const uint32_t idesc = idesc_bf16_f32(kBlockRows, kBatch);
                 const uint32_t d = tmem + (uint32_t)(s * kBatch);
                 const uint64_t a0 = smem_desc_k16(sm.A[0]), a1 = smem_desc_k16(sm.A[1]), a2 = smem_desc_k16(sm.A[2]);
@@ -408,13 +417,19 @@ struct Producer {
     }
 };
 
+// Resident CTAs per SM requested from the register allocator.  The SIMT variant needs
+// no tensor-core operand tiles and fits 8 CTAs (40 warps) per SM at 48 registers; the
+// tensor-core variant runs 5 (its shared memory allows 6).
+constexpr int kCtaMinBlocksSimt = 8;
+constexpr int kCtaMinBlocksTc = 5;
+
 template <bool TC, bool COUNT>
-__global__ void __launch_bounds__(kBlockRows + 32) k_forward_cta(
+__global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMinBlocksSimt) k_forward_cta(
     const float4* __restrict__ s_sorted, int64_t S, const uint2* __restrict__ bdesc,
     const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes, const GaussRec* __restrict__ recs,
     float* __restrict__ out_cells, float* __restrict__ out_weights, int* status, unsigned long long* stats) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smem_raw);
+    CtaSmem<TC>& sm = *reinterpret_cast<CtaSmem<TC>*>(smem_raw);
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int64_t blk = blockIdx.x;
     const uint2 bd = bdesc[blk];
@@ -437,7 +452,7 @@ __global__ void __launch_bounds__(kBlockRows + 32) k_forward_cta(
 
     if (w == 4) {
         // ---------------- producer ----------------
-        Producer<TC, COUNT> pr{sm, recs, status, tmem, 0u, false, 0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, {}, false};
+        Producer<TC, COUNT> pr{sm, recs, status, tmem, 0u, false, 0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, false};
         TravCount tc;
         int st = 0;
         for (int g = 0; g < ng && !pr.failed; g++) {
@@ -462,8 +477,9 @@ __global__ void __launch_bounds__(kBlockRows + 32) k_forward_cta(
                 const bool in = row < S && r >= ra && r < rb;
                 float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (in) p = s_sorted[row];
-                pr.wb[q] = warp_box6(in, p.x, p.y, p.z);
-                if (TC) {
+                const Box6 bq = warp_box6(in, p.x, p.y, p.z);
+                if (lane == 0) sm.wb[q] = bq;
+                if constexpr (TC) {
                     float phi[16];
                     const float ux = in ? p.x - pr.x0 : 0.f, uy = in ? p.y - pr.y0 : 0.f, uz = in ? p.z - pr.z0 : 0.f;
                     phi[0] = ux * ux;
@@ -515,7 +531,7 @@ __global__ void __launch_bounds__(kBlockRows + 32) k_forward_cta(
         if (valid) spv = s_sorted[row];
         const float x = spv.x, y = spv.y, z = spv.z;
         float W = 0.f, V = 0.f;
-        int ncand = 0, ncontrib = 0;
+        int ncand = 0, ncontrib = 0, nlane = 0;
         uint32_t n = 0;  // batches consumed
         while (true) {
             const int stage = (int)(n % kStages);
@@ -527,6 +543,7 @@ __global__ void __launch_bounds__(kBlockRows + 32) k_forward_cta(
             const bool ing = valid && t >= ra && t < rb;
             const uint8_t cm = sm.colmask[stage][lane];
             const uint32_t wm = __ballot_sync(0xffffffffu, (cm >> w) & 1u);
+            if (COUNT) nlane += 32 * __popc(wm);
             if (TC) {
                 const uint32_t fb = __ballot_sync(0xffffffffu, (cm >> 4) & 1u);
                 tc_fence_after();
@@ -602,6 +619,7 @@ __global__ void __launch_bounds__(kBlockRows + 32) k_forward_cta(
             if (lane == 0) {
                 atomicAdd(&stats[0], a);
                 atomicAdd(&stats[1], b);
+                atomicAdd(&stats[9], (unsigned long long)nlane);
             }
         }
     }
@@ -625,7 +643,7 @@ cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32
 
 template <bool TC, bool COUNT>
 static cudaError_t launch_cta_impl(const CtaArgs& a, cudaStream_t st) {
-    const size_t smem = sizeof(CtaSmem) + 1024;
+    const size_t smem = sizeof(CtaSmem<TC>) + 1024;
     cudaError_t e = cudaFuncSetAttribute(k_forward_cta<TC, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;

@@ -115,7 +115,9 @@ struct gvc_ctx {
                             // (32 if unused), byte 3 = number of groups
     gvc::DevBuf blk_desc;   // [ceil(S/128)] uint2 block-group descriptors (CTA kernels)
     gvc::DevBuf blk_boxes;  // [ceil(S/128) * 8] block-group boxes, 2 x float4
-    gvc::DevBuf s_grad;     // [n_tiles*32] float4 (out, outw, dL_dout, dL_doutw) for the backward
+    gvc::DevBuf s_grad;     // [n_tiles*32] float4 (x, y, z, gx) backward sample records
+    gvc::DevBuf s_gyz;      // [n_tiles*32] float gyz (see k_sample_grads)
+    gvc::DevBuf s_ok;       // [n_tiles*32] uint8 1 iff W > 0.01 (pair statistics only)
     gvc::Lbvh s_sort;       // sample sort (keys/perm only)
     gvc::Lbvh tiles;        // tile LBVH
     // Gaussian state (forward)

@@ -274,23 +274,36 @@ __global__ void __launch_bounds__(256) k_sample_tiles(int64_t S, int64_t n_tiles
 
 // Per sorted sample: (gO / W, -gO * out / W, gW, 1) if W > 0.01, else zeros
 // (backward.cu:260-263 and :268-279).
+// Backward sample records in sorted order: (x, y, z, gx) with gx = dL/dout / W, gyz =
+// -dL/dout * out / W + dL/dW (backward.cu:252-298 folds the same factors per pair), and
+// ok = W > 0.01.  Samples below the cutoff get gx = gyz = 0, so their pairs add exactly
+// nothing; tile padding gets finite coordinates (0) and zero gradients for the same reason.
 __global__ void __launch_bounds__(256) k_sample_grads(int64_t n_slots, const float4* __restrict__ s_sorted,
                                                       const float* __restrict__ out_cells,
                                                       const float* __restrict__ out_weights,
                                                       const float* __restrict__ gout, const float* __restrict__ gw,
-                                                      float4* __restrict__ s_grad) {
+                                                      float4* __restrict__ s_grad, float* __restrict__ s_gyz,
+                                                      uint8_t* __restrict__ s_ok) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n_slots) return;
-    const int o = __float_as_int(s_sorted[i].w);
+    const float4 sp = s_sorted[i];
+    const int o = __float_as_int(sp.w);
+    float gx = 0.f, gyz = 0.f;
+    uint8_t ok = 0;
     float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
     if (o >= 0) {
         const float W = out_weights[o];
         if (W > kWeightCutoff) {
             const float g = gout[o];
-            r = make_float4(g / W, -(g * out_cells[o]) / W, gw[o], 1.f);
+            gx = g / W;
+            gyz = -(g * out_cells[o]) / W + gw[o];
+            ok = 1;
         }
+        r = make_float4(sp.x, sp.y, sp.z, gx);
     }
     s_grad[i] = r;
+    s_gyz[i] = gyz;
+    s_ok[i] = ok;
 }
 
 static inline unsigned nb256(int64_t n) { return (unsigned)((n + 255) / 256); }
@@ -321,9 +334,10 @@ cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples
 
 cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float* out_cells,
                                 const float* out_weights, const float* gout, const float* gw, float4* s_grad,
-                                cudaStream_t st) {
+                                float* s_gyz, uint8_t* s_ok, cudaStream_t st) {
     if (n_slots <= 0) return cudaSuccess;
-    k_sample_grads<<<nb256(n_slots), 256, 0, st>>>(n_slots, s_sorted, out_cells, out_weights, gout, gw, s_grad); gvc::note_launch();
+    k_sample_grads<<<nb256(n_slots), 256, 0, st>>>(n_slots, s_sorted, out_cells, out_weights, gout, gw, s_grad,
+                                                   s_gyz, s_ok); gvc::note_launch();
     return cudaGetLastError();
 }
 

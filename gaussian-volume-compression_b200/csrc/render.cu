@@ -8,9 +8,9 @@
 // sample against each of them, accumulating W and V in registers (no atomics).
 //
 // Backward, deterministic (replaces BACKWARD::renderCUDA, backward.cu:127-337): one
-// warp per Gaussian walks the sample-tile LBVH with the Gaussian's AABB; lanes are the
-// tile's samples; per-lane partial sums are reduced once per Gaussian (a fixed-order
-// segmented reduction, no atomics).
+// warp per Gaussian walks the sample-group LBVH with the Gaussian's AABB; the rows of the
+// candidate groups are packed densely onto the lanes; per-lane partial moments are
+// reduced once per Gaussian (a fixed-order segmented reduction, no atomics).
 //
 // Backward, atomic (replaces BACKWARD::sampleRenderCUDA, backward.cu:339-559): one warp
 // per sample tile re-walks the Gaussian LBVH; the 11 per-pair terms are pre-reduced over
@@ -165,128 +165,226 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_forward(const float4* _
 }
 
 // --------------------------------------------------------------------------------
-// Backward helpers: the per-pair adjoint of one (sample, Gaussian) pair.
-//   sample grad record sg = (gO/W, -gO*out/W, gW, ok) with ok = 1 iff W > 0.01.
-//   acc: 0 dv, 1 dw, 2..4 dmean, 5..10 dconic (unique parameters, off-diagonals x2).
+// Backward pair math.  For a pair (sample x, Gaussian g) with d = x - mu and the base-2
+// power p2 evaluated exactly as in the forward (same staged coefficients, same window),
+// e = 2^p2 and gs = (v gx + gyz) e, the Gaussian accumulates eleven moments
+//   m0 = sum gx e, m1 = sum gs, m2..4 = sum gs d, m5..10 = sum gs (dx dx, dx dy, dx dz, dy dy, dy dz, dz dz)
+// and moments_to_terms() turns them into the per-Gaussian sums of backward.cu:252-298:
+//   dL/dv = w m0, dL/dw = m1, dL/dmu = w C (m2, m3, m4),
+//   dL/dconic (unique entries, off-diagonals counted twice) = -w/2 m5, -w m6, -w m7, -w/2 m8, -w m9, -w/2 m10.
+// The weight w and the conic multiply once per Gaussian instead of once per pair.
 // --------------------------------------------------------------------------------
-struct GaussParams {
-    float mx, my, mz, w, v;
-    float c0, c1, c2, c3, c4, c5;
-    float4 lo, hi;
+struct GaussB {
+    float mx, my, mz, v;
+    float q0, q1, q2, q3, q4, q5;  // base-2 power coefficients, off-diagonals doubled
+    float lx, ly, lz, hx, hy, hz;  // AABB
 };
 
-__device__ __forceinline__ bool pair_adjoint(const GaussParams& g, float4 sp, float4 sg, float (&acc)[16]) {
-    if (!(g.lo.x <= sp.x && sp.x <= g.hi.x && g.lo.y <= sp.y && sp.y <= g.hi.y && g.lo.z <= sp.z && sp.z <= g.hi.z))
-        return false;
-    if (sg.w == 0.0f) return false;
-    const float dx = sp.x - g.mx, dy = sp.y - g.my, dz = sp.z - g.mz;
-    const float t0 = g.c0 * dx + g.c1 * dy + g.c2 * dz;
-    const float t1 = g.c1 * dx + g.c3 * dy + g.c4 * dz;
-    const float t2 = g.c2 * dx + g.c4 * dy + g.c5 * dz;
-    const float p = -0.5f * (dx * t0 + dy * t1 + dz * t2);
-    if (p < kPowerFloor || p > 0.0f) return false;
-    const float e = __expf(p);
-    const float wt = g.w * e;
-    acc[0] += sg.x * wt;                       // dL/dv = gO * wt / W
-    const float gsum = g.v * sg.x + sg.y + sg.z;  // gO (v - out) / W + gW
-    acc[1] += gsum * e;                        // dL/dw
-    const float gw = gsum * wt;                // = -2 dL/dquad
-    acc[2] += gw * t0;
-    acc[3] += gw * t1;
-    acc[4] += gw * t2;
-    const float dq = -0.5f * gw;               // dL/dquad
-    acc[5] += dq * dx * dx;
-    acc[6] += dq * 2.0f * dx * dy;
-    acc[7] += dq * 2.0f * dx * dz;
-    acc[8] += dq * dy * dy;
-    acc[9] += dq * 2.0f * dy * dz;
-    acc[10] += dq * dz * dz;
-    return true;
+__device__ __forceinline__ GaussB gauss_b(float mx, float my, float mz, float v, float c0, float c1, float c2,
+                                          float c3, float c4, float c5, float4 lo, float4 hi) {
+    GaussB g;
+    g.mx = mx; g.my = my; g.mz = mz; g.v = v;
+    g.q0 = kHalfLog2e * c0;
+    g.q1 = 2.f * (kHalfLog2e * c1);
+    g.q2 = 2.f * (kHalfLog2e * c2);
+    g.q3 = kHalfLog2e * c3;
+    g.q4 = 2.f * (kHalfLog2e * c4);
+    g.q5 = kHalfLog2e * c5;
+    g.lx = lo.x; g.ly = lo.y; g.lz = lo.z;
+    g.hx = hi.x; g.hy = hi.y; g.hz = hi.z;
+    return g;
+}
+
+// p = (x, y, z, gx) with finite coordinates; gx = gyz = 0 makes every term exactly 0.
+// Branch-free: a pair outside the box or the power window gets e = 0.  Returns whether
+// the pair is inside the box and the window.
+__device__ __forceinline__ bool pair_moments(const GaussB& g, float4 p, float gyz, float (&m)[11]) {
+    const bool in = g.lx <= p.x && p.x <= g.hx && g.ly <= p.y && p.y <= g.hy && g.lz <= p.z && p.z <= g.hz;
+    const float dx = p.x - g.mx, dy = p.y - g.my, dz = p.z - g.mz;
+    const float p2 = dx * fmaf(g.q0, dx, fmaf(g.q1, dy, g.q2 * dz)) + dy * fmaf(g.q3, dy, g.q4 * dz) + dz * (g.q5 * dz);
+    const bool c = in && p2 >= kLog2Floor && p2 <= 0.0f;
+    const float e = c ? ex2_approx(p2) : 0.0f;
+    m[0] = fmaf(p.w, e, m[0]);
+    const float gs = fmaf(g.v, p.w, gyz) * e;
+    m[1] += gs;
+    const float gx = gs * dx, gy = gs * dy, gz = gs * dz;
+    m[2] += gx;
+    m[3] += gy;
+    m[4] += gz;
+    m[5] = fmaf(gx, dx, m[5]);
+    m[6] = fmaf(gx, dy, m[6]);
+    m[7] = fmaf(gx, dz, m[7]);
+    m[8] = fmaf(gy, dy, m[8]);
+    m[9] = fmaf(gy, dz, m[9]);
+    m[10] = fmaf(gz, dz, m[10]);
+    return c;
+}
+
+// After warp_transpose_reduce16 lanes 2k, 2k+1 hold moment k; returns gradient field k
+// (0 dv, 1 dw, 2..4 dmean, 5..10 dconic; 0 for k >= 11).  Warp-collective.
+__device__ __forceinline__ float moments_to_terms(float tot, float w, float c0, float c1, float c2, float c3,
+                                                  float c4, float c5) {
+    const int k = (threadIdx.x & 31) >> 1;
+    const float a2 = __shfl_sync(0xffffffffu, tot, 4), a3 = __shfl_sync(0xffffffffu, tot, 6),
+                a4 = __shfl_sync(0xffffffffu, tot, 8);
+    if (k == 0) return w * tot;
+    if (k == 1) return tot;
+    if (k == 2) return w * (c0 * a2 + c1 * a3 + c2 * a4);
+    if (k == 3) return w * (c1 * a2 + c3 * a3 + c4 * a4);
+    if (k == 4) return w * (c2 * a2 + c4 * a3 + c5 * a4);
+    if (k == 5 || k == 8 || k == 10) return -0.5f * w * tot;
+    if (k == 6 || k == 7 || k == 9) return -w * tot;
+    return 0.f;
 }
 
 // --------------------------------------------------------------------------------
-// Backward, deterministic Gaussian-owned segmented reduction.
+// Backward, deterministic Gaussian-owned reduction with densely packed sample rows.
 // --------------------------------------------------------------------------------
-// Gaussian-owned visitor: the warp's lanes are the samples of each candidate group; two
-// groups are evaluated per step (their loads issued together, two independent
-// dependency chains per lane).
-struct BwdGaussVisitor {
-    const float4* __restrict__ s_sorted;
-    const float4* __restrict__ s_grad;
-    const uint32_t* __restrict__ gdesc;
-    GaussParams g;
-    float acc[16];
-    int npairs;
+// A candidate leaf is one lane group of a sample tile (rows [start, end) of the tile).
+// Groups hold 1..32 rows, so mapping lanes to a group's rows leaves lanes idle; instead
+// the rows of successive candidate groups are appended to a per-warp ring and evaluated
+// kFlush at a time (kRowsPerLane rows per lane, all loads issued before the arithmetic:
+// the kernel is bound by the latency of these gathers).  The order in which rows reach
+// lanes depends only on the traversal order, so the sums are deterministic.
+constexpr int kRowsPerLane = 2;
+constexpr int kFlush = 32 * kRowsPerLane;  // rows per evaluation
+constexpr int kRing = 2 * kFlush;          // queued rows stay below kFlush + 32
 
-    // leaf l = (tile l / kGroups, group l % kGroups): lanes [start, end) of the tile
-    __device__ __forceinline__ void load(int l, int lane, float4& sp, float4& sg, bool& in) const {
-        const int64_t t = l / kGroups;
-        const int gi = l % kGroups;
-        const uint32_t gd = __ldg(gdesc + t);
-        const int start = gi == 0 ? 0 : (int)((gd >> (8 * (gi - 1))) & 0xffu);
-        const int end = gi < 3 ? (int)((gd >> (8 * gi)) & 0xffu) : 32;
-        in = lane >= start && lane < end;
-        sp = __ldg(s_sorted + t * 32 + lane);
-        sg = __ldg(s_grad + t * 32 + lane);
+template <bool COUNT>
+struct BwdDenseVisitor {
+    const float4* __restrict__ s_grad;
+    const float* __restrict__ s_gyz;
+    const uint8_t* __restrict__ s_ok;
+    const uint32_t* __restrict__ gdesc;
+    int* ring;     // shared [kRing]
+    int4* leaves;  // shared [32]: (first slot of tile, start lane, end lane, rows queued through this leaf)
+    uint32_t head, tail;
+    GaussB g;
+    float m[11];
+    int npairs;
+    int nrows;  // rows evaluated (warp-uniform, statistics)
+
+    // evaluates the n (1..kFlush) rows at the ring head
+    __device__ __forceinline__ void eval(int n) {
+        const int lane = threadIdx.x & 31;
+        float4 p[kRowsPerLane];
+        float y[kRowsPerLane];
+        int r[kRowsPerLane];
+#pragma unroll
+        for (int k = 0; k < kRowsPerLane; k++) {
+            p[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            y[k] = 0.f;
+            r[k] = -1;
+            if (lane + 32 * k < n) {
+                r[k] = ring[(head + (uint32_t)(32 * k + lane)) & (kRing - 1)];
+                p[k] = __ldg(s_grad + r[k]);
+                y[k] = __ldg(s_gyz + r[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kRowsPerLane; k++) {
+            if (32 * k < n) {
+                const bool c = pair_moments(g, p[k], y[k], m);
+                if (COUNT && c && r[k] >= 0 && s_ok[r[k]]) npairs++;
+            }
+        }
+        if (COUNT) nrows += n;
+        head += (uint32_t)n;
     }
 
     __device__ __forceinline__ void operator()(const int* c, int nb) {
         const int lane = threadIdx.x & 31;
-        for (int i = 0; i < nb; i += 2) {
-            float4 sp0, sg0, sp1, sg1;
-            bool in0, in1;
-            load(c[i], lane, sp0, sg0, in0);
-            load(c[min(i + 1, nb - 1)], lane, sp1, sg1, in1);
-            in1 = in1 && (i + 1 < nb);
-            if (in0) npairs += pair_adjoint(g, sp0, sg0, acc) ? 1 : 0;
-            if (in1) npairs += pair_adjoint(g, sp1, sg1, acc) ? 1 : 0;
+        int sz = 0;
+        int4 L = make_int4(0, 0, 0, 0);
+        if (lane < nb) {
+            const int leaf = c[lane];
+            const int t = leaf >> 2;  // leaf = tile * kGroups + group
+            const int gi = leaf & 3;
+            const uint32_t gd = __ldg(gdesc + t);
+            const int start = gi == 0 ? 0 : (int)((gd >> (8 * (gi - 1))) & 0xffu);
+            const int end = gi < 3 ? (int)((gd >> (8 * gi)) & 0xffu) : 32;
+            sz = end - start;
+            L = make_int4(t * 32, start, end, 0);
+        }
+        int incl = sz;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += v;
+        }
+        L.w = incl;
+        leaves[lane] = L;
+        __syncwarp();
+        const uint32_t base = tail;
+        for (int j = 0; j < nb; j++) {
+            const int4 q = leaves[j];
+            const int excl = q.w - (q.z - q.y);
+            if (lane >= q.y && lane < q.z) ring[(base + (uint32_t)(excl + lane - q.y)) & (kRing - 1)] = q.x + lane;
+            if (base + (uint32_t)q.w - head >= (uint32_t)kFlush) {
+                __syncwarp();
+                eval(kFlush);
+            }
+        }
+        tail = base + (uint32_t)__shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();
+    }
+
+    __device__ __forceinline__ void drain() {
+        while (tail != head) {
+            __syncwarp();
+            const uint32_t n = tail - head;
+            eval(n < (uint32_t)kFlush ? (int)n : kFlush);
         }
         __syncwarp();
     }
 };
 
+// Warps (consecutive Gaussians in Morton order) per block: neighbouring Gaussians gather
+// overlapping sample rows, which then hit in the SM's L1.
+constexpr int kBwdWarps = 4;
+
 template <bool COUNT>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_gauss(
+__global__ void __launch_bounds__(kBwdWarps * 32) k_backward_gauss(
     int P, const int32_t* __restrict__ gorder, const float* __restrict__ means, const float* __restrict__ values,
     const float* __restrict__ weights, const float* __restrict__ conics, const float4* __restrict__ boxes,
-    const float4* __restrict__ s_sorted, const float4* __restrict__ s_grad, const uint32_t* __restrict__ gdesc,
-    const BvhNode* __restrict__ tnodes, float* __restrict__ gacc, int* status, unsigned long long* stats) {
-    __shared__ int s_stack[kWarpsPerBlock][kStackCap];
-    __shared__ int s_cand[kWarpsPerBlock][kCandCap];
+    const float4* __restrict__ s_grad, const float* __restrict__ s_gyz, const uint8_t* __restrict__ s_ok,
+    const uint32_t* __restrict__ gdesc, const BvhNode* __restrict__ tnodes, float* __restrict__ gacc, int* status,
+    unsigned long long* stats) {
+    __shared__ int s_stack[kBwdWarps][kStackCap];
+    __shared__ int s_cand[kBwdWarps][kCandCap];
+    __shared__ int s_ring[kBwdWarps][kRing];
+    __shared__ int4 s_leaves[kBwdWarps][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gi = blockIdx.x * kWarpsPerBlock + warp;
+    const int gi = blockIdx.x * kBwdWarps + warp;
     if (gi >= P) return;
-    const int o = gorder ? gorder[gi] : gi;
-    BwdGaussVisitor vis;
-    vis.s_sorted = s_sorted;
+    const int64_t o = gorder ? gorder[gi] : gi;
+    BwdDenseVisitor<COUNT> vis;
     vis.s_grad = s_grad;
+    vis.s_gyz = s_gyz;
+    vis.s_ok = s_ok;
     vis.gdesc = gdesc;
-
-    vis.g.mx = __ldg(means + 3 * (int64_t)o);
-    vis.g.my = __ldg(means + 3 * (int64_t)o + 1);
-    vis.g.mz = __ldg(means + 3 * (int64_t)o + 2);
-    vis.g.w = __ldg(weights + o);
-    vis.g.v = __ldg(values + o);
-    vis.g.c0 = __ldg(conics + 6 * (int64_t)o);
-    vis.g.c1 = __ldg(conics + 6 * (int64_t)o + 1);
-    vis.g.c2 = __ldg(conics + 6 * (int64_t)o + 2);
-    vis.g.c3 = __ldg(conics + 6 * (int64_t)o + 3);
-    vis.g.c4 = __ldg(conics + 6 * (int64_t)o + 4);
-    vis.g.c5 = __ldg(conics + 6 * (int64_t)o + 5);
-    vis.g.lo = __ldg(boxes + 2 * (int64_t)o);
-    vis.g.hi = __ldg(boxes + 2 * (int64_t)o + 1);
+    vis.ring = s_ring[warp];
+    vis.leaves = s_leaves[warp];
+    vis.head = vis.tail = 0u;
+    const float* cp = conics + 6 * o;
+    const float4 lo = __ldg(boxes + 2 * o), hi = __ldg(boxes + 2 * o + 1);
+    vis.g = gauss_b(__ldg(means + 3 * o), __ldg(means + 3 * o + 1), __ldg(means + 3 * o + 2), __ldg(values + o),
+                    __ldg(cp), __ldg(cp + 1), __ldg(cp + 2), __ldg(cp + 3), __ldg(cp + 4), __ldg(cp + 5), lo, hi);
 #pragma unroll
-    for (int k = 0; k < 16; k++) vis.acc[k] = 0.f;
+    for (int k = 0; k < 11; k++) vis.m[k] = 0.f;
     vis.npairs = 0;
+    vis.nrows = 0;
     TravCount tc;
-    const int st = warp_traverse(tnodes, make_float3(vis.g.lo.x, vis.g.lo.y, vis.g.lo.z),
-                                 make_float3(vis.g.hi.x, vis.g.hi.y, vis.g.hi.z), s_stack[warp], s_cand[warp], vis,
-                                 tc);
-    const float tot = warp_transpose_reduce16(vis.acc);
-    if (!(lane & 1)) {
-        const int k = lane >> 1;  // value index held by this lane
-        gacc[16 * (int64_t)o + k] = tot;
-    }
+    const int st = warp_traverse(tnodes, make_float3(lo.x, lo.y, lo.z), make_float3(hi.x, hi.y, hi.z), s_stack[warp],
+                                 s_cand[warp], vis, tc);
+    vis.drain();
+    float v16[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) v16[k] = k < 11 ? vis.m[k] : 0.f;
+    const float tot = warp_transpose_reduce16(v16);
+    const float term = moments_to_terms(tot, __ldg(weights + o), __ldg(cp), __ldg(cp + 1), __ldg(cp + 2),
+                                        __ldg(cp + 3), __ldg(cp + 4), __ldg(cp + 5));
+    if (!(lane & 1)) gacc[16 * o + (lane >> 1)] = term;
     if (st && lane == 0) atomicOr(status, st);
     if (COUNT) {
         unsigned long long a = (unsigned long long)vis.npairs;
@@ -296,6 +394,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_gauss(
             atomicMax(&stats[4], (unsigned long long)tc.max_sp);
             atomicAdd(&stats[7], (unsigned long long)tc.leaves);
             atomicAdd(&stats[8], (unsigned long long)tc.nodes);
+            atomicAdd(&stats[10], (unsigned long long)vis.nrows);
         }
     }
 }
@@ -307,7 +406,10 @@ struct BwdTileVisitor {
     const GaussRec* __restrict__ recs;
     const int32_t* __restrict__ gperm;
     float4* batch;  // shared [32 * 5]
-    float4 sp, sg;
+    float4 p;       // (x, y, z, gx); gx = 0 outside the current group
+    float gyz;      // 0 outside the current group
+    bool act;       // lane in the current group
+    bool ok;
     float* __restrict__ gacc;
     int npairs;
 
@@ -324,24 +426,23 @@ struct BwdTileVisitor {
         __syncwarp();
         for (int gi = 0; gi < nb; gi++) {
             const float4 r0 = batch[gi * 5 + 0], r1 = batch[gi * 5 + 1], r2 = batch[gi * 5 + 2];
-            GaussParams g;
-            g.mx = r0.x; g.my = r0.y; g.mz = r0.z; g.w = r0.w;
-            g.c0 = r1.x; g.c1 = r1.y; g.c2 = r1.z; g.c3 = r1.w;
-            g.c4 = r2.x; g.c5 = r2.y; g.v = r2.z;
-            g.lo = batch[gi * 5 + 3];
-            g.hi = batch[gi * 5 + 4];
-            float acc[16];
+            const GaussB g = gauss_b(r0.x, r0.y, r0.z, r2.z, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, batch[gi * 5 + 3],
+                                     batch[gi * 5 + 4]);
+            float m[11];
 #pragma unroll
-            for (int k = 0; k < 16; k++) acc[k] = 0.f;
-            const bool hit = pair_adjoint(g, sp, sg, acc);
-            const uint32_t any = __ballot_sync(0xffffffffu, hit);
-            if (any == 0u) continue;
-            npairs += hit ? 1 : 0;
-            const float tot = warp_transpose_reduce16(acc);
+            for (int k = 0; k < 11; k++) m[k] = 0.f;
+            const bool hit = pair_moments(g, p, gyz, m) && act;
+            if (!__any_sync(0xffffffffu, hit)) continue;
+            npairs += (hit && ok) ? 1 : 0;
+            float v16[16];
+#pragma unroll
+            for (int k = 0; k < 16; k++) v16[k] = k < 11 ? m[k] : 0.f;
+            const float tot = warp_transpose_reduce16(v16);
+            const float term = moments_to_terms(tot, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y);
             const int k = lane >> 1;
             if (!(lane & 1) && k < 11) {
                 const int o = gperm[c[gi]];
-                atomicAdd(gacc + 16 * (int64_t)o + k, tot);
+                atomicAdd(gacc + 16 * (int64_t)o + k, term);
             }
         }
         __syncwarp();
@@ -350,10 +451,10 @@ struct BwdTileVisitor {
 
 template <bool COUNT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_tiles(
-    const float4* __restrict__ s_sorted, const float4* __restrict__ s_grad, const float4* __restrict__ group_boxes,
-    const uint32_t* __restrict__ gdesc, int n_tiles, const BvhNode* __restrict__ gnodes,
-    const GaussRec* __restrict__ recs, const int32_t* __restrict__ gperm, float* __restrict__ gacc, int* status,
-    unsigned long long* stats) {
+    const float4* __restrict__ s_grad, const float* __restrict__ s_gyz, const uint8_t* __restrict__ s_ok,
+    const float4* __restrict__ group_boxes, const uint32_t* __restrict__ gdesc, int n_tiles,
+    const BvhNode* __restrict__ gnodes, const GaussRec* __restrict__ recs, const int32_t* __restrict__ gperm,
+    float* __restrict__ gacc, int* status, unsigned long long* stats) {
     __shared__ int s_stack[kWarpsPerBlock][kStackCap];
     __shared__ int s_cand[kWarpsPerBlock][kCandCap];
     __shared__ float4 s_batch[kWarpsPerBlock][32 * 5];
@@ -364,9 +465,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_tiles(
     vis.recs = recs;
     vis.gperm = gperm;
     vis.batch = s_batch[warp];
-    const float4 sp = s_sorted[(int64_t)tile * 32 + lane];
-    const float4 sg = s_grad[(int64_t)tile * 32 + lane];
-    vis.sp = sp;
+    const int64_t slot = (int64_t)tile * 32 + lane;
+    const float4 sp = s_grad[slot];
+    const float syz = s_gyz[slot];
+    vis.ok = s_ok[slot] != 0;
     vis.gacc = gacc;
     vis.npairs = 0;
     const uint32_t gd = gdesc[tile];
@@ -374,10 +476,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_backward_tiles(
     TravCount tc;
     int st = 0;
     for (int g = 0; g < ng; g++) {
-        const int64_t slot = (int64_t)tile * kGroups + g;
-        const float4 tlo = group_boxes[2 * slot], thi = group_boxes[2 * slot + 1];
-        // lanes outside the group see ok = 0 and contribute nothing
-        vis.sg = mygroup == g ? sg : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int64_t gslot = (int64_t)tile * kGroups + g;
+        const float4 tlo = group_boxes[2 * gslot], thi = group_boxes[2 * gslot + 1];
+        // lanes outside the group carry zero gradients and are not counted
+        vis.act = mygroup == g;
+        vis.p = make_float4(sp.x, sp.y, sp.z, vis.act ? sp.w : 0.f);
+        vis.gyz = vis.act ? syz : 0.f;
         st |= warp_traverse(gnodes, make_float3(tlo.x, tlo.y, tlo.z), make_float3(thi.x, thi.y, thi.z),
                             s_stack[warp], s_cand[warp], vis, tc);
     }
@@ -566,12 +670,12 @@ cudaError_t launch_forward(const FwdArgs& a, cudaStream_t st) {
 cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st) {
     if (a.P <= 0) return cudaSuccess;
     if (a.count) {
-        k_backward_gauss<true><<<nblk(a.P, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_sorted, a.s_grad, a.gdesc,
+        k_backward_gauss<true><<<nblk(a.P, kBwdWarps), kBwdWarps * 32, 0, st>>>(
+            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_grad, a.s_gyz, a.s_ok, a.gdesc,
             a.tnodes, a.gacc, a.status, a.stats);
     } else {
-        k_backward_gauss<false><<<nblk(a.P, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_sorted, a.s_grad, a.gdesc,
+        k_backward_gauss<false><<<nblk(a.P, kBwdWarps), kBwdWarps * 32, 0, st>>>(
+            (int)a.P, a.gorder, a.means, a.values, a.weights, a.conics, a.boxes, a.s_grad, a.s_gyz, a.s_ok, a.gdesc,
             a.tnodes, a.gacc, a.status, a.stats);
     }
     gvc::note_launch();
@@ -582,11 +686,11 @@ cudaError_t launch_backward_tiles(const BwdArgs& a, cudaStream_t st) {
     if (a.n_tiles <= 0) return cudaSuccess;
     if (a.count) {
         k_backward_tiles<true><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            a.s_sorted, a.s_grad, a.tile_boxes, a.gdesc, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc,
+            a.s_grad, a.s_gyz, a.s_ok, a.tile_boxes, a.gdesc, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc,
             a.status, a.stats);
     } else {
         k_backward_tiles<false><<<nblk(a.n_tiles, kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(
-            a.s_sorted, a.s_grad, a.tile_boxes, a.gdesc, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc,
+            a.s_grad, a.s_gyz, a.s_ok, a.tile_boxes, a.gdesc, (int)a.n_tiles, a.gnodes, a.recs, a.gperm, a.gacc,
             a.status, a.stats);
     }
     gvc::note_launch();

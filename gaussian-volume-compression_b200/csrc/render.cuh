@@ -29,7 +29,9 @@ struct BwdArgs {
     const float* conics;
     const float4* boxes;  // caller order, lo/hi
     const float4* s_sorted;
-    const float4* s_grad;
+    const float4* s_grad;      // (x, y, z, gx) per sorted slot
+    const float* s_gyz;        // gyz per sorted slot
+    const uint8_t* s_ok;       // W > 0.01 per sorted slot (pair statistics)
     const float4* tile_boxes;  // group boxes [n_tiles * kGroups]
     const uint32_t* gdesc;     // [n_tiles]
     int64_t n_tiles;
@@ -79,7 +81,7 @@ cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples
                                 uint32_t* gdesc, cudaStream_t st);
 cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float* out_cells,
                                 const float* out_weights, const float* gout, const float* gw, float4* s_grad,
-                                cudaStream_t st);
+                                float* s_gyz, uint8_t* s_ok, cudaStream_t st);
 cudaError_t launch_fill_zero_outputs(int64_t S, float* out_cells, float* out_weights, cudaStream_t st);
 
 // mesh.cu

@@ -58,7 +58,8 @@ class GvcStats(ctypes.Structure):
                 ("bwd_kernel_ms", ctypes.c_double), ("fwd_kernel_calls", ctypes.c_int64),
                 ("bwd_kernel_calls", ctypes.c_int64), ("fwd_leaf_hits", ctypes.c_int64),
                 ("fwd_node_visits", ctypes.c_int64), ("bwd_leaf_hits", ctypes.c_int64),
-                ("bwd_node_visits", ctypes.c_int64)]
+                ("bwd_node_visits", ctypes.c_int64), ("fwd_lane_evals", ctypes.c_int64),
+                ("bwd_rows", ctypes.c_int64)]
 
 
 _lib = None

@@ -71,6 +71,8 @@ typedef struct {
     int64_t fwd_node_visits;  /* internal LBVH nodes popped by the forward traversal        */
     int64_t bwd_leaf_hits;    /* (Gaussian or tile) leaves evaluated by the backward        */
     int64_t bwd_node_visits;
+    int64_t fwd_lane_evals;   /* (sample, Gaussian) lane slots the forward evaluated (CTA paths) */
+    int64_t bwd_rows;         /* (sample, Gaussian) rows the deterministic backward evaluated   */
 } gvc_stats;
 
 /* Context: owns the sample ordering, both LBVHs and all workspace (no per-call
