@@ -36,6 +36,7 @@ CONFIGS = {
     "large": (2_000_000, 16_000_000, "large evaluation: 2M clustered Gaussians x 16M points (8M uniform + 8M near means)"),
     "medium": (200_000, 4_000_000, "scaled large evaluation: 200k clustered Gaussians x 4M points"),
     "small": (200_000, 2_000_000, "profiling case: 200k clustered Gaussians x 2M points"),
+    "slice": (2_000_000, 4_000_000, "profiling case with the large evaluation's Gaussians: 2M clustered Gaussians x 4M points"),
 }
 METRIC = "fwd+bwd ms/step (2M Gaussians×16M pts), TC vs plain FP32 at stated FP64 err"
 # Algorithmic FP32 work per pair (FORWARD forward.cu:224-256, BACKWARD backward.cu:252-298):

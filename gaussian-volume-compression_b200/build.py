@@ -27,6 +27,7 @@ SOURCES = {
     "mesh.cu": ["--fmad=false"],
     "noalloc.cu": [],
     "cta.cu": [],
+    "bwd_tc.cu": [],
 }
 
 

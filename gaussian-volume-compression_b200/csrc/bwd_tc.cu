@@ -1,0 +1,396 @@
+// bwd_tc.cu -- backward of the mixture field on 128-sample blocks with the per-Gaussian
+// reduction over samples on the tensor cores (replaces BACKWARD::sampleRenderCUDA,
+// diff-gaussian-rasterization/cuda_rasterizer/backward.cu:339-559: sample-side
+// traversal, per-Gaussian sums added atomically).
+//
+// One CTA owns the 128 Morton-sorted samples of a block and the block groups of the
+// forward (k_sample_blocks).  A producer warp walks the Gaussian LBVH once per group and
+// hands out the candidate Gaussians 128 at a time; consumer thread t owns candidate t of
+// a batch (and TMEM lane t).  For a group with centre x0 and a sample row with u = x - x0,
+//   phi(u) = [1, ux, uy, uz, ux ux, ux uy, ux uz, uy uy, uy uz, uz uz]
+//   Psi(row) = [gx phi(u), gyz phi(u), 0 x 12]                     (B: 32 x rows)
+// and with e the pair's exponential (the forward's base-2 power, window and AABB test),
+//   D[gaussian][k] = sum over rows of e(row, gaussian) Psi(row)[k]  (A = E: 128 x rows)
+// is one GEMM per batch, accumulated in FP32 in tensor memory by tcgen05.mma (M = 128,
+// N = 32, K = 16 rows per chunk).  E and Psi are split into three BF16 parts each and the
+// six products with i + j <= 2 are accumulated (about 24 bits).  Thread t then reads its
+// own row of D, turns the moments about x0 into the moments about its mean (pair.cuh)
+// and adds its eleven gradient terms with FP32 atomics.  An MMA warp issues the products
+// while the consumers compute the next 16-row chunk (two A buffers).
+#include "pair.cuh"
+#include "render.cuh"
+#include "tc.cuh"
+#include "traverse.cuh"
+
+namespace gvc {
+
+constexpr int kBRows = 128;            // sample rows per block (the forward's blocks)
+constexpr int kBGroups = 8;            // block groups per block
+constexpr int kBBatch = 128;           // candidate Gaussians per batch (consumer threads)
+constexpr int kBStages = 2;            // candidate batches in flight
+constexpr int kBChunks = kBRows / 16;  // K chunks of 16 rows
+constexpr int kMom = 32;               // B rows: 20 moment features + zero padding
+constexpr int kPsiStride = 21;         // floats per row of the per-warp Psi scratch
+
+struct BwdSmem {
+    unsigned char A[2][3][kBBatch * 32];        // E chunk (128 x 16 bf16), three parts, two buffers
+    unsigned char B[kBChunks][3][kMom * 32];    // Psi (32 x 16 bf16) per chunk, three parts
+    float psi[4][32 * kPsiStride];              // per consumer warp: Psi of its 32 rows (fp32)
+    float4 rows[kBRows];                        // (x, y, z, W > 0.01) of the block's rows
+    int cand[kBStages][kBBatch];                // candidate Gaussians (LBVH leaf = record index)
+    int2 desc[kBStages];                        // (count or -1 at the end, group)
+    int stack[kStackCap];
+    int tcand[kCandCap];
+    uint64_t full[kBStages], empty[kBStages], aready[2], afree[2], dready, dfree;
+    uint32_t tmem_base;
+};
+
+__device__ __forceinline__ int bgroup_start(uint2 d, int g) {
+    if (g == 0) return 0;
+    if (g >= kBGroups) return kBRows;
+    if (g <= 4) return (int)((d.x >> (8 * (g - 1))) & 0xffu);
+    return (int)((d.y >> (8 * (g - 5))) & 0xffu);
+}
+
+// Producer: collects candidates into 128-entry batches (stage n % kBStages for batch n).
+struct BwdProducer {
+    BwdSmem& sm;
+    int* status;
+    uint32_t total;  // batches published
+    int fill;        // entries in the open batch
+    int g;           // current group
+    bool failed;
+
+    __device__ __forceinline__ bool acquire(uint32_t n) {
+        const uint32_t k = n / kBStages;
+        if (k == 0) return true;
+        return mbar_wait(&sm.empty[n % kBStages], (k - 1) & 1u, status);
+    }
+
+    __device__ __forceinline__ void publish(int count) {
+        const int lane = threadIdx.x & 31;
+        __syncwarp();
+        if (lane == 0) {
+            sm.desc[total % kBStages] = make_int2(count, g);
+            mbar_arrive(&sm.full[total % kBStages]);
+        }
+        total++;
+        fill = 0;
+        if (!acquire(total)) failed = true;
+        __syncwarp();
+    }
+
+    __device__ __forceinline__ void operator()(const int* c, int nb) {
+        const int lane = threadIdx.x & 31;
+        int done = 0;
+        while (done < nb && !failed) {
+            const int take = min(nb - done, kBBatch - fill);
+            if (lane < take) sm.cand[total % kBStages][fill + lane] = c[done + lane];
+            fill += take;
+            done += take;
+            if (fill == kBBatch) publish(kBBatch);
+        }
+        __syncwarp();
+    }
+};
+
+// Splits 16 fp32 values into three bf16 parts and stores them as row r of the three tiles.
+__device__ __forceinline__ void store_split_row(unsigned char* t0, unsigned char* t1, unsigned char* t2, int r,
+                                                const float (&v)[16]) {
+    __nv_bfloat16 h[16], m[16], l[16];
+    split_bf16(v, h, m, l);
+    store_row_k16(t0, r, h);
+    store_row_k16(t1, r, m);
+    store_row_k16(t2, r, l);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kBRows + 64, 3) k_backward_cta(
+    int64_t n_slots, const uint2* __restrict__ bdesc, const float4* __restrict__ bboxes,
+    const BvhNode* __restrict__ gnodes, const GaussRec* __restrict__ recs, const int32_t* __restrict__ gperm,
+    const float4* __restrict__ s_grad, const float* __restrict__ s_gyz, const uint8_t* __restrict__ s_ok,
+    float* __restrict__ gacc, int* status, unsigned long long* stats) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    BwdSmem& sm = *reinterpret_cast<BwdSmem*>(smem_raw);
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+    const int64_t blk = blockIdx.x;
+    const uint2 bd = bdesc[blk];
+    const int ng = (int)(bd.y >> 24);
+    if (t == 0) {
+        for (int s = 0; s < kBStages; s++) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 4);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&sm.aready[b], 4);
+            mbar_init(&sm.afree[b], 1);
+        }
+        mbar_init(&sm.dready, 1);
+        mbar_init(&sm.dfree, 4);
+        fence_mbar_init();
+    }
+    if (t < kBRows) {
+        const int64_t row = blk * kBRows + t;
+        float4 p = make_float4(NAN, NAN, NAN, 0.f);
+        if (row < n_slots) {
+            const float4 q = s_grad[row];
+            p = make_float4(q.x, q.y, q.z, s_ok[row] ? 1.f : 0.f);
+        }
+        sm.rows[t] = p;
+    }
+    if (w == 0) {
+        tmem_alloc(&sm.tmem_base, 32);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem_base;
+
+    if (w == 4) {
+        // ---------------- producer ----------------
+        BwdProducer pr{sm, status, 0u, 0, 0, false};
+        TravCount tc;
+        int st = 0;
+        for (int g = 0; g < ng && !pr.failed; g++) {
+            pr.g = g;
+            const float4 glo = bboxes[2 * (blk * kBGroups + g)], ghi = bboxes[2 * (blk * kBGroups + g) + 1];
+            st |= warp_traverse(gnodes, make_float3(glo.x, glo.y, glo.z), make_float3(ghi.x, ghi.y, ghi.z), sm.stack,
+                                sm.tcand, pr, tc);
+            if (pr.fill > 0 && !pr.failed) pr.publish(pr.fill);
+        }
+        if (lane == 0) {
+            if (st) atomicOr(status, st);
+            if (!pr.failed) {
+                sm.desc[pr.total % kBStages] = make_int2(-1, 0);
+                mbar_arrive(&sm.full[pr.total % kBStages]);
+            }
+            if (COUNT) {
+                atomicMax(&stats[4], (unsigned long long)tc.max_sp);
+                atomicAdd(&stats[7], (unsigned long long)tc.leaves);
+                atomicAdd(&stats[8], (unsigned long long)tc.nodes);
+            }
+        }
+        __syncwarp();
+    } else if (w == 5) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16_f32(kBBatch, kMom);
+            uint32_t j = 0;  // chunk counter (same sequence as the consumers)
+            for (uint32_t n = 0;; n++) {
+                const int s = (int)(n % kBStages);
+                if (!mbar_wait(&sm.full[s], (n / kBStages) & 1u, status)) break;
+                const int2 d = sm.desc[s];
+                if (d.x < 0) break;
+                const int ra = bgroup_start(bd, d.y), rb = bgroup_start(bd, d.y + 1);
+                const int q0 = ra >> 4, q1 = (rb - 1) >> 4;
+                if (n > 0 && !mbar_wait(&sm.dfree, (n - 1) & 1u, status)) break;
+                bool ok = true;
+                for (int q = q0; q <= q1; q++, j++) {
+                    const int b = (int)(j & 1u);
+                    if (!mbar_wait(&sm.aready[b], (j >> 1) & 1u, status)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t a0 = smem_desc_k16(sm.A[b][0]), a1 = smem_desc_k16(sm.A[b][1]),
+                                   a2 = smem_desc_k16(sm.A[b][2]);
+                    const uint64_t b0 = smem_desc_k16(sm.B[q][0]), b1 = smem_desc_k16(sm.B[q][1]),
+                                   b2 = smem_desc_k16(sm.B[q][2]);
+                    umma_bf16(tmem, a2, b0, idesc, q == q0 ? 0u : 1u);  // lo * hi
+                    umma_bf16(tmem, a1, b1, idesc, 1u);                 // mid * mid
+                    umma_bf16(tmem, a0, b2, idesc, 1u);                 // hi * lo
+                    umma_bf16(tmem, a1, b0, idesc, 1u);                 // mid * hi
+                    umma_bf16(tmem, a0, b1, idesc, 1u);                 // hi * mid
+                    umma_bf16(tmem, a0, b0, idesc, 1u);                 // hi * hi
+                    umma_commit(&sm.afree[b]);
+                }
+                if (!ok) break;
+                umma_commit(&sm.dready);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- consumers: thread t owns candidate t of each batch ----------------
+        float* psi = sm.psi[w];
+        int cur_group = -1;
+        float x0 = 0.f, y0 = 0.f, z0 = 0.f;
+        uint32_t j = 0;
+        int ncand = 0, ncontrib = 0;
+        long long nlane = 0;  // lane slots evaluated (warp-uniform)
+        for (uint32_t n = 0;; n++) {
+            const int s = (int)(n % kBStages);
+            const bool okw = mbar_wait(&sm.full[s], (n / kBStages) & 1u, status);
+            if (!__all_sync(0xffffffffu, okw)) break;
+            const int2 d = sm.desc[s];
+            if (d.x < 0) break;
+            const int ra = bgroup_start(bd, d.y), rb = bgroup_start(bd, d.y + 1);
+            const int q0 = ra >> 4, q1 = (rb - 1) >> 4;
+            if (d.y != cur_group) {
+                // Psi of this warp's rows (chunks 2w, 2w + 1) for the new group; every MMA of
+                // the previous group has completed (dready of its last batch was awaited).
+                cur_group = d.y;
+                const float4 glo = bboxes[2 * (blk * kBGroups + d.y)], ghi = bboxes[2 * (blk * kBGroups + d.y) + 1];
+                x0 = 0.5f * (glo.x + ghi.x);
+                y0 = 0.5f * (glo.y + ghi.y);
+                z0 = 0.5f * (glo.z + ghi.z);
+                const int r = 32 * w + lane;
+                const bool in = r >= ra && r < rb && blk * kBRows + r < n_slots;
+                float gx = 0.f, gyz = 0.f, ux = 0.f, uy = 0.f, uz = 0.f;
+                if (in) {
+                    const float4 q = s_grad[blk * kBRows + r];
+                    gx = q.w;
+                    gyz = s_gyz[blk * kBRows + r];
+                    ux = q.x - x0;
+                    uy = q.y - y0;
+                    uz = q.z - z0;
+                }
+                const float ph[10] = {1.f, ux, uy, uz, ux * ux, ux * uy, ux * uz, uy * uy, uy * uz, uz * uz};
+#pragma unroll
+                for (int k = 0; k < 10; k++) {
+                    psi[lane * kPsiStride + k] = in ? gx * ph[k] : 0.f;
+                    psi[lane * kPsiStride + 10 + k] = in ? gyz * ph[k] : 0.f;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    // tile row (feature) = lane of chunk 2w + h
+                    float v[16];
+#pragma unroll
+                    for (int k = 0; k < 16; k++) v[k] = lane < 20 ? psi[(16 * h + k) * kPsiStride + lane] : 0.f;
+                    const int q = 2 * w + h;
+                    store_split_row(sm.B[q][0], sm.B[q][1], sm.B[q][2], lane, v);
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+            }
+            // this thread's Gaussian (an empty box when the batch is not full)
+            float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0, r2 = r0;
+            float4 blo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), bhi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+            int leaf = -1;
+            if (t < d.x) {
+                leaf = sm.cand[s][t];
+                const float4* rp = reinterpret_cast<const float4*>(recs + leaf);
+                r0 = __ldg(rp);
+                r1 = __ldg(rp + 1);
+                r2 = __ldg(rp + 2);
+                blo = __ldg(rp + 3);
+                bhi = __ldg(rp + 4);
+            }
+            const GaussB g = gauss_b(r0.x, r0.y, r0.z, r2.z, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, blo, bhi);
+            bool anyc = false;
+            bool okc = true;
+            for (int q = q0; q <= q1; q++, j++) {
+                const int b = (int)(j & 1u);
+                if (j >= 2) {
+                    const bool okf = mbar_wait(&sm.afree[b], ((j >> 1) - 1) & 1u, status);
+                    if (!__all_sync(0xffffffffu, okf)) {
+                        okc = false;
+                        break;
+                    }
+                }
+                float e[16];
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const int r = 16 * q + k;
+                    const float4 p = sm.rows[r];
+                    const bool in = r >= ra && r < rb && g.lx <= p.x && p.x <= g.hx && g.ly <= p.y && p.y <= g.hy &&
+                                    g.lz <= p.z && p.z <= g.hz;
+                    e[k] = 0.f;
+                    if (__any_sync(0xffffffffu, in)) {
+                        const float dx = p.x - g.mx, dy = p.y - g.my, dz = p.z - g.mz;
+                        const float p2 = dx * fmaf(g.q0, dx, fmaf(g.q1, dy, g.q2 * dz)) +
+                                         dy * fmaf(g.q3, dy, g.q4 * dz) + dz * (g.q5 * dz);
+                        const bool c = in && p2 >= kLog2Floor && p2 <= 0.0f;
+                        e[k] = c ? ex2_approx(p2) : 0.f;
+                        anyc |= c;
+                        if (COUNT) {
+                            ncand += in ? 1 : 0;
+                            ncontrib += (c && p.w != 0.f) ? 1 : 0;
+                            nlane += 32;
+                        }
+                    }
+                }
+                tc_fence_after();
+                store_split_row(sm.A[b][0], sm.A[b][1], sm.A[b][2], t, e);
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&sm.aready[b]);
+            }
+            if (!okc) break;
+            const bool okd = mbar_wait(&sm.dready, n & 1u, status);
+            if (!__all_sync(0xffffffffu, okd)) break;
+            tc_fence_after();
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(32 * w) << 16), v);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&sm.dfree);
+                mbar_arrive(&sm.empty[s]);
+            }
+            if (anyc) {
+                // moments about the group centre -> moments about the mean (d = u - a)
+                const float ax = g.mx - x0, ay = g.my - y0, az = g.mz - z0;
+                float S[10];
+#pragma unroll
+                for (int k = 0; k < 10; k++) S[k] = fmaf(g.v, v[k], v[10 + k]);
+                float m[11];
+                m[0] = v[0];
+                m[1] = S[0];
+                m[2] = S[1] - ax * S[0];
+                m[3] = S[2] - ay * S[0];
+                m[4] = S[3] - az * S[0];
+                m[5] = S[4] - 2.f * ax * S[1] + ax * ax * S[0];
+                m[6] = S[5] - ax * S[2] - ay * S[1] + ax * ay * S[0];
+                m[7] = S[6] - ax * S[3] - az * S[1] + ax * az * S[0];
+                m[8] = S[7] - 2.f * ay * S[2] + ay * ay * S[0];
+                m[9] = S[8] - ay * S[3] - az * S[2] + ay * az * S[0];
+                m[10] = S[9] - 2.f * az * S[3] + az * az * S[0];
+                float tm[11];
+                moments_to_terms_lane(m, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, tm);
+                float* dst = gacc + 16 * (int64_t)gperm[leaf];
+#pragma unroll
+                for (int k = 0; k < 11; k++) atomicAdd(dst + k, tm[k]);
+            }
+        }
+        if (COUNT) {
+            unsigned long long a = (unsigned long long)ncand, c = (unsigned long long)ncontrib;
+            for (int off = 16; off > 0; off >>= 1) {
+                a += __shfl_xor_sync(0xffffffffu, a, off);
+                c += __shfl_xor_sync(0xffffffffu, c, off);
+            }
+            (void)a;
+            if (lane == 0) {
+                atomicAdd(&stats[2], c);
+                atomicAdd(&stats[10], (unsigned long long)nlane);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (w == 0) tmem_dealloc(tmem, 32);
+}
+
+template <bool COUNT>
+static cudaError_t launch_bwd_cta_impl(const BwdArgs& a, int64_t n_blocks, const uint2* bdesc, const float4* bboxes,
+                                       cudaStream_t st) {
+    const size_t smem = sizeof(BwdSmem) + 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_backward_cta<COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_backward_cta<COUNT><<<(unsigned)n_blocks, kBRows + 64, smem, st>>>(
+        a.n_tiles * kTile, bdesc, bboxes, a.gnodes, a.recs, a.gperm, a.s_grad, a.s_gyz, a.s_ok, a.gacc, a.status,
+        a.stats);
+    gvc::note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward_cta(const BwdArgs& a, int64_t n_blocks, const uint2* bdesc, const float4* bboxes,
+                                cudaStream_t st) {
+    if (n_blocks <= 0 || a.P <= 0) return cudaSuccess;
+    return a.count ? launch_bwd_cta_impl<true>(a, n_blocks, bdesc, bboxes, st)
+                   : launch_bwd_cta_impl<false>(a, n_blocks, bdesc, bboxes, st);
+}
+
+}  // namespace gvc

@@ -409,6 +409,9 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
     GVC_CUDA(sc->gacc.ensure(sizeof(float) * 16 * P), "alloc gacc");
     float* gacc = sc->gacc.as<float>();
     const bool atomic_mode = ctx->bwd_mode == 2 || (ctx->bwd_mode == 0 && use_gaussian_bvh);
+    // the tensor-core path reduces over samples on tcgen05 (atomic accumulation) unless the
+    // deterministic reduction is forced
+    const bool tc_bwd = ctx->eval_path == 1 && ctx->bwd_mode != 1;
     const bool have_order = ctx->gauss_ready && ctx->P == P;
     if (ctx->n_tiles == 0) {
         GVC_CUDA(cudaMemsetAsync(gacc, 0, sizeof(float) * 16 * P, st), "zero gacc");
@@ -441,7 +444,23 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
         ba.stats = ctx->d_stats;
         ba.count = ctx->count_pairs != 0;
         tm.mark();
-        if (atomic_mode) {
+        if (tc_bwd) {
+            if (!have_order) GVC_CUDA(lbvh_build_boxes(ctx->gbvh, P, boxes, st), "Gaussian LBVH");
+            GVC_CUDA(ctx->grec.ensure(sizeof(GaussRec) * P), "alloc records");
+            GVC_CUDA(launch_gather_recs(P, ctx->gbvh.perm.as<int32_t>(), means3D, values, weights, conics, boxes,
+                                        ctx->grec.as<GaussRec>(), st),
+                     "gather records");
+            GVC_CUDA(cudaMemsetAsync(gacc, 0, sizeof(float) * 16 * P, st), "zero gacc");
+            ba.gorder = nullptr;
+            ba.gperm = ctx->gbvh.perm.as<int32_t>();
+            ba.gnodes = ctx->gbvh.nodes.as<BvhNode>();
+            ba.recs = ctx->grec.as<GaussRec>();
+            const int tk = timer_begin(ctx, st, 1);
+            GVC_CUDA(launch_backward_cta(ba, (S + 127) / 128, ctx->blk_desc.as<uint2>(), ctx->blk_boxes.as<float4>(),
+                                         st),
+                     "backward (tensor core)");
+            timer_end(ctx, st, tk);
+        } else if (atomic_mode) {
             if (!have_order) GVC_CUDA(lbvh_build_boxes(ctx->gbvh, P, boxes, st), "Gaussian LBVH");
             GVC_CUDA(ctx->grec.ensure(sizeof(GaussRec) * P), "alloc records");
             GVC_CUDA(launch_gather_recs(P, ctx->gbvh.perm.as<int32_t>(), means3D, values, weights, conics, boxes,

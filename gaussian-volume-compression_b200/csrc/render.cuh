@@ -65,6 +65,9 @@ cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32
 cudaError_t launch_forward_cta(const CtaArgs& a, bool tc, cudaStream_t st);
 cudaError_t launch_tc_gemm_test(const void* A, const void* B, int N, float* D, int* status, cudaStream_t st);
 cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st);
+// bwd_tc.cu: backward on 128-sample blocks with the reduction over samples on tcgen05
+cudaError_t launch_backward_cta(const BwdArgs& a, int64_t n_blocks, const uint2* bdesc, const float4* bboxes,
+                                cudaStream_t st);
 cudaError_t launch_backward_tiles(const BwdArgs& a, cudaStream_t st);
 cudaError_t launch_finalize(int64_t P, const float* gacc, const float* scales, const float* rots, const float* conics,
                             float sm, int ref_compat, float* dmeans, float* dscales, float* drots, float* dvalues,
