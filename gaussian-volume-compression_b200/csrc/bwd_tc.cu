@@ -30,12 +30,10 @@ constexpr int kBBatch = 128;           // candidate Gaussians per batch (consume
 constexpr int kBStages = 2;            // candidate batches in flight
 constexpr int kBChunks = kBRows / 16;  // K chunks of 16 rows
 constexpr int kMom = 32;               // B rows: 20 moment features + zero padding
-constexpr int kPsiStride = 21;         // floats per row of the per-warp Psi scratch
 
 struct BwdSmem {
     unsigned char A[2][3][kBBatch * 32];        // E chunk (128 x 16 bf16), three parts, two buffers
     unsigned char B[kBChunks][3][kMom * 32];    // Psi (32 x 16 bf16) per chunk, three parts
-    float psi[4][32 * kPsiStride];              // per consumer warp: Psi of its 32 rows (fp32)
     float4 rows[kBRows];                        // (x, y, z, W > 0.01) of the block's rows
     int cand[kBStages][kBBatch];                // candidate Gaussians (LBVH leaf = record index)
     int2 desc[kBStages];                        // (count or -1 at the end, group)
@@ -105,7 +103,7 @@ __device__ __forceinline__ void store_split_row(unsigned char* t0, unsigned char
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(kBRows + 64, 3) k_backward_cta(
+__global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     int64_t n_slots, const uint2* __restrict__ bdesc, const float4* __restrict__ bboxes,
     const BvhNode* __restrict__ gnodes, const GaussRec* __restrict__ recs, const int32_t* __restrict__ gperm,
     const float4* __restrict__ s_grad, const float* __restrict__ s_gyz, const uint8_t* __restrict__ s_ok,
@@ -129,6 +127,10 @@ __global__ void __launch_bounds__(kBRows + 64, 3) k_backward_cta(
         mbar_init(&sm.dfree, 4);
         fence_mbar_init();
     }
+    // features 20..31 of every Psi tile stay zero
+    for (int i = t; i < (int)(sizeof(sm.B) / sizeof(uint4)); i += kBRows + 64)
+        reinterpret_cast<uint4*>(&sm.B[0][0][0])[i] = make_uint4(0u, 0u, 0u, 0u);
+    fence_proxy_async_smem();
     if (t < kBRows) {
         const int64_t row = blk * kBRows + t;
         float4 p = make_float4(NAN, NAN, NAN, 0.f);
@@ -212,7 +214,6 @@ __global__ void __launch_bounds__(kBRows + 64, 3) k_backward_cta(
         __syncwarp();
     } else {
         // ---------------- consumers: thread t owns candidate t of each batch ----------------
-        float* psi = sm.psi[w];
         int cur_group = -1;
         float x0 = 0.f, y0 = 0.f, z0 = 0.f;
         uint32_t j = 0;
@@ -246,20 +247,20 @@ __global__ void __launch_bounds__(kBRows + 64, 3) k_backward_cta(
                     uz = q.z - z0;
                 }
                 const float ph[10] = {1.f, ux, uy, uz, ux * ux, ux * uy, ux * uz, uy * uy, uy * uz, uz * uz};
+                // row r is column k = r % 16 of chunk r / 16; feature n is tile row n
+                const int q = r >> 4, k = r & 15;
+                const int koff = (k >> 3) * 128 + (k & 7) * 2;
 #pragma unroll
-                for (int k = 0; k < 10; k++) {
-                    psi[lane * kPsiStride + k] = in ? gx * ph[k] : 0.f;
-                    psi[lane * kPsiStride + 10 + k] = in ? gyz * ph[k] : 0.f;
-                }
-                __syncwarp();
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    // tile row (feature) = lane of chunk 2w + h
-                    float v[16];
-#pragma unroll
-                    for (int k = 0; k < 16; k++) v[k] = lane < 20 ? psi[(16 * h + k) * kPsiStride + lane] : 0.f;
-                    const int q = 2 * w + h;
-                    store_split_row(sm.B[q][0], sm.B[q][1], sm.B[q][2], lane, v);
+                for (int n = 0; n < 20; n++) {
+                    const float v = in ? (n < 10 ? gx : gyz) * ph[n < 10 ? n : n - 10] : 0.f;
+                    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+                    const float r1 = v - __bfloat162float(h);
+                    const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+                    const __nv_bfloat16 l = __float2bfloat16_rn(r1 - __bfloat162float(m));
+                    const int off = (n >> 3) * 256 + (n & 7) * 16 + koff;
+                    *reinterpret_cast<__nv_bfloat16*>(sm.B[q][0] + off) = h;
+                    *reinterpret_cast<__nv_bfloat16*>(sm.B[q][1] + off) = m;
+                    *reinterpret_cast<__nv_bfloat16*>(sm.B[q][2] + off) = l;
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
@@ -349,9 +350,10 @@ __global__ void __launch_bounds__(kBRows + 64, 3) k_backward_cta(
                 m[10] = S[9] - 2.f * az * S[3] + az * az * S[0];
                 float tm[11];
                 moments_to_terms_lane(m, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, tm);
-                float* dst = gacc + 16 * (int64_t)gperm[leaf];
-#pragma unroll
-                for (int k = 0; k < 11; k++) atomicAdd(dst + k, tm[k]);
+                float4* dst = reinterpret_cast<float4*>(gacc + 16 * (int64_t)gperm[leaf]);
+                atomicAdd(dst, make_float4(tm[0], tm[1], tm[2], tm[3]));
+                atomicAdd(dst + 1, make_float4(tm[4], tm[5], tm[6], tm[7]));
+                atomicAdd(dst + 2, make_float4(tm[8], tm[9], tm[10], 0.f));
             }
         }
         if (COUNT) {
