@@ -45,6 +45,13 @@ F_FWD_CONTRIB = 28     # + w e, two accumulations (contributing pair, plus one E
 F_BWD_CONTRIB = 64     # recompute + adjoint (contributing pair with W > 0.01, plus one EX2)
 EX2_EQUIV = 8          # MUFU ex2 issue cost in FP32-lane units (16/clk/SM vs 128/clk/SM)
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant
+# kernels at the 2M x 16M workload, from one single-pass capture of
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
+#  -k regex:"k_backward_gauss|k_forward_cta" -s 2 -c 2 python bench.py --profile --steps 1 --warmup 1`;
+# other workloads report null.
+MEASURED_TRAFFIC = {("large", "k_backward_gauss"): 1.475e9 + 0.125e9,
+                    ("large", "k_forward_cta"): 1.416e9 + 0.934e9}
 
 
 def parse():
@@ -311,13 +318,19 @@ def run_ours(args):
     t_fwd = kt["fwd_kernel_ms"] / max(kt["fwd_kernel_calls"], 1)
     t_bwd = kt["bwd_kernel_ms"] / max(kt["bwd_kernel_calls"], 1)
     hbm, bf16, bf16s, src = measured_peaks()
+    bwd_kernel = "k_backward_cta" if args.eval_path == "tensor_core" and args.bwd_mode != "deterministic" else (
+        "k_backward_tiles" if args.bwd_mode == "atomic" or (args.bwd_mode == "auto" and ugb) else "k_backward_gauss")
+    fwd_kernel = "k_forward" if args.eval_path == "plain_tile" else "k_forward_cta"
     if t_bwd >= t_fwd:
-        name, flops, t_k = "k_backward_gauss (Gaussian-owned adjoint)", f_bwd, t_bwd
+        name, flops, t_k = bwd_kernel, f_bwd, t_bwd
     else:
-        name, flops, t_k = "k_forward (tile traversal + evaluation)", f_fwd, t_fwd
+        name, flops, t_k = fwd_kernel, f_fwd, t_fwd
+    traffic = MEASURED_TRAFFIC.get((args.config, name))
     achieved = flops / (t_k * 1e-3) / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                "frac": achieved / bf16, "traffic": None, "kernel": name, "kernel_ms": t_k,
+                "frac": achieved / bf16, "traffic": traffic, "kernel": name, "kernel_ms": t_k,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size launch"
+                                  if traffic else None,
                 "peak_source": "%s bf16 dense (MEASURED_PEAKS.json)" % src,
                 "fp32_simt_nominal_tflops": FP32_NOMINAL_TFLOPS,
                 "frac_of_fp32_simt_nominal": achieved / FP32_NOMINAL_TFLOPS,
