@@ -250,11 +250,16 @@ static void grid_build(orc_grid* g, int64_t n, const float* boxes, const double 
     for (int a = 0; a < 3; a++) hmax = fmax(hmax, (ghi[a] - glo[a]) / 1000.0);
     if (!(h > hmax)) h = hmax;
     if (!(h > 0)) h = 1.0;
-    g->inv_h = 1.0 / h;
-    for (int a = 0; a < 3; a++) {
-        g->lo[a] = glo[a];
-        g->n[a] = (int64_t)floor((ghi[a] - glo[a]) * g->inv_h) + 1;
-        if (g->n[a] < 1) g->n[a] = 1;
+    /* at most ~64 grid cells per item (degenerate boxes would otherwise ask for 1e9) */
+    for (;;) {
+        g->inv_h = 1.0 / h;
+        for (int a = 0; a < 3; a++) {
+            g->lo[a] = glo[a];
+            g->n[a] = (int64_t)floor((ghi[a] - glo[a]) * g->inv_h) + 1;
+            if (g->n[a] < 1) g->n[a] = 1;
+        }
+        if ((double)g->n[0] * (double)g->n[1] * (double)g->n[2] <= 64.0 * (double)n + 4096.0) break;
+        h *= 1.5;
     }
     int64_t ncell = g->n[0] * g->n[1] * g->n[2];
     int64_t* cnt = (int64_t*)calloc((size_t)ncell + 1, sizeof(int64_t));
