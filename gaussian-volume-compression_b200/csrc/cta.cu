@@ -281,7 +281,7 @@ __device__ __forceinline__ void cp_async_wait() {
 // its records are copied into shared memory with cp.async as soon as the traversal hands
 // them over, and the batch is finalised (coefficients, masks, MMAs) one call later, while
 // the next batch's copies are in flight.
-template <bool TC, bool COUNT>
+template <bool TC, bool COUNT, int NCW>
 struct Producer {
     CtaSmem<TC>& sm;
     const GaussRec* __restrict__ recs;
@@ -313,7 +313,7 @@ struct Producer {
             sm.gd[s][lane][1] = make_float4(c0, 2.f * c1, 2.f * c2, c3);
             sm.gd[s][lane][2] = make_float4(2.f * c4, c5, r2.z, 0.f);
 #pragma unroll
-            for (int ww = 0; ww < 4; ww++) cm |= overlap6(sm.wb[ww], r3, r4) ? (uint8_t)(1u << ww) : (uint8_t)0;
+            for (int ww = 0; ww < NCW; ww++) cm |= overlap6(sm.wb[ww], r3, r4) ? (uint8_t)(1u << ww) : (uint8_t)0;
             if constexpr (TC) {
                 const float mx = r0.x - x0, my = r0.y - y0, mz = r0.z - z0;
                 const float cmx = c0 * mx + c1 * my + c2 * mz;
@@ -417,19 +417,28 @@ struct Producer {
     }
 };
 
-// Resident CTAs per SM requested from the register allocator.  The SIMT variant needs
-// no tensor-core operand tiles and fits 8 CTAs (40 warps) per SM at 48 registers; the
-// tensor-core variant runs 5 (its shared memory allows 6).
-constexpr int kCtaMinBlocksSimt = 8;
+// Resident CTAs per SM requested from the register allocator.  The tensor-core variant
+// (4 consumer warps, one row per thread) runs 5 (its shared memory allows 6); the SIMT
+// variant with one row per thread fits 8 (40 warps), with two rows per thread 16
+// (48 warps, 40 registers).
 constexpr int kCtaMinBlocksTc = 5;
+constexpr int kCtaMinBlocksSimt1 = 8;
+constexpr int kCtaMinBlocksSimt2 = 16;
+// Rows per consumer thread of the SIMT variant: each staged record (80 bytes broadcast to
+// every lane) then serves two samples, halving the shared-memory datapath traffic.
+constexpr int kSimtRowsPerThread = 2;
 
-template <bool TC, bool COUNT>
-__global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMinBlocksSimt) k_forward_cta(
+template <bool TC, bool COUNT, int RPT>
+__global__ void __launch_bounds__((4 / RPT) * 32 + 32,
+                                  TC ? kCtaMinBlocksTc : (RPT == 1 ? kCtaMinBlocksSimt1 : kCtaMinBlocksSimt2))
+    k_forward_cta(
     const float4* __restrict__ s_sorted, int64_t S, const uint2* __restrict__ bdesc,
     const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes, const GaussRec* __restrict__ recs,
     float* __restrict__ out_cells, float* __restrict__ out_weights, int* status, unsigned long long* stats) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     CtaSmem<TC>& sm = *reinterpret_cast<CtaSmem<TC>*>(smem_raw);
+    static_assert(!TC || RPT == 1, "the tensor-core variant owns one row (TMEM lane) per thread");
+    constexpr int NCW = 4 / RPT;  // consumer warps; warp NCW is the producer
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int64_t blk = blockIdx.x;
     const uint2 bd = bdesc[blk];
@@ -437,7 +446,7 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
     if (t == 0) {
         for (int s = 0; s < kStages; s++) {
             mbar_init(&sm.full[s], 2);
-            mbar_init(&sm.empty[s], 4);
+            mbar_init(&sm.empty[s], NCW);
         }
         fence_mbar_init();
     }
@@ -450,9 +459,9 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
     if (TC) tc_fence_after();
     const uint32_t tmem = TC ? sm.tmem_base : 0u;
 
-    if (w == 4) {
+    if (w == NCW) {
         // ---------------- producer ----------------
-        Producer<TC, COUNT> pr{sm, recs, status, tmem, 0u, false, 0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, false};
+        Producer<TC, COUNT, NCW> pr{sm, recs, status, tmem, 0u, false, 0, 0, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, false};
         TravCount tc;
         int st = 0;
         for (int g = 0; g < ng && !pr.failed; g++) {
@@ -472,13 +481,26 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
             if (TC) tc_fence_after();
 #pragma unroll
             for (int q = 0; q < 4; q++) {
+                // row r belongs to consumer warp q / RPT
                 const int r = 32 * q + lane;
                 const int64_t row = blk * kBlockRows + r;
                 const bool in = row < S && r >= ra && r < rb;
                 float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (in) p = s_sorted[row];
                 const Box6 bq = warp_box6(in, p.x, p.y, p.z);
-                if (lane == 0) sm.wb[q] = bq;
+                if (lane == 0) {
+                    if (q % RPT == 0) {
+                        sm.wb[q / RPT] = bq;
+                    } else {
+                        Box6& u = sm.wb[q / RPT];
+                        u.lx = fminf(u.lx, bq.lx);
+                        u.ly = fminf(u.ly, bq.ly);
+                        u.lz = fminf(u.lz, bq.lz);
+                        u.hx = fmaxf(u.hx, bq.hx);
+                        u.hy = fmaxf(u.hy, bq.hy);
+                        u.hz = fmaxf(u.hz, bq.hz);
+                    }
+                }
                 if constexpr (TC) {
                     float phi[16];
                     const float ux = in ? p.x - pr.x0 : 0.f, uy = in ? p.y - pr.y0 : 0.f, uz = in ? p.z - pr.z0 : 0.f;
@@ -524,13 +546,23 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
             atomicAdd(&stats[6], (unsigned long long)tc.nodes);
         }
     } else {
-        // ---------------- consumers ----------------
-        const int64_t row = blk * kBlockRows + t;
-        const bool valid = row < S;
-        float4 spv = make_float4(NAN, NAN, NAN, __int_as_float(-1));
-        if (valid) spv = s_sorted[row];
-        const float x = spv.x, y = spv.y, z = spv.z;
-        float W = 0.f, V = 0.f;
+        // ---------------- consumers: thread (w, lane) owns rows (w * RPT + k) * 32 + lane ----------------
+        float xr[RPT], yr[RPT], zr[RPT], Wr[RPT], Vr[RPT];
+        int orig[RPT];
+        bool valid[RPT];
+#pragma unroll
+        for (int k = 0; k < RPT; k++) {
+            const int64_t row = blk * kBlockRows + (w * RPT + k) * 32 + lane;
+            valid[k] = row < S;
+            float4 spv = make_float4(NAN, NAN, NAN, __int_as_float(-1));
+            if (valid[k]) spv = s_sorted[row];
+            xr[k] = spv.x;
+            yr[k] = spv.y;
+            zr[k] = spv.z;
+            orig[k] = __float_as_int(spv.w);
+            Wr[k] = 0.f;
+            Vr[k] = 0.f;
+        }
         int ncand = 0, ncontrib = 0, nlane = 0;
         uint32_t n = 0;  // batches consumed
         while (true) {
@@ -540,11 +572,18 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
             const int2 d = sm.desc[stage];
             if (d.x < 0) break;
             const int ra = group_start(bd, d.y), rb = group_start(bd, d.y + 1);
-            const bool ing = valid && t >= ra && t < rb;
+            bool ing[RPT];
+#pragma unroll
+            for (int k = 0; k < RPT; k++) {
+                const int r = (w * RPT + k) * 32 + lane;
+                ing[k] = valid[k] && r >= ra && r < rb;
+            }
             const uint8_t cm = sm.colmask[stage][lane];
             const uint32_t wm = __ballot_sync(0xffffffffu, (cm >> w) & 1u);
-            if (COUNT) nlane += 32 * __popc(wm);
-            if (TC) {
+            if (COUNT) nlane += 32 * RPT * __popc(wm);
+            if constexpr (TC) {
+                const float x = xr[0], y = yr[0], z = zr[0];
+                float W = Wr[0], V = Vr[0];
                 const uint32_t fb = __ballot_sync(0xffffffffu, (cm >> 4) & 1u);
                 tc_fence_after();
                 float v[32];
@@ -553,7 +592,7 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
                 for (int j = 0; j < kBatch; j++) {
                     if (!((wm >> j) & 1u)) continue;
                     const float4 lo = sm.gd[stage][j][3], hi = sm.gd[stage][j][4];
-                    const bool in = ing && lo.x <= x && x <= hi.x && lo.y <= y && y <= hi.y && lo.z <= z && z <= hi.z;
+                    const bool in = ing[0] && lo.x <= x && x <= hi.x && lo.y <= y && y <= hi.y && lo.z <= z && z <= hi.z;
                     const float4 r0 = sm.gd[stage][j][0];
                     float p2 = v[j];
                     if ((fb >> j) & 1u) {
@@ -571,6 +610,8 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
                         ncontrib += cc ? 1 : 0;
                     }
                 }
+                Wr[0] = W;
+                Vr[0] = V;
                 tc_fence_before();
             } else {
                 uint32_t mm = wm;
@@ -578,18 +619,23 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
                     const int j = __ffs(mm) - 1;
                     mm &= mm - 1;
                     const float4 lo = sm.gd[stage][j][3], hi = sm.gd[stage][j][4];
-                    const bool in = ing && lo.x <= x && x <= hi.x && lo.y <= y && y <= hi.y && lo.z <= z && z <= hi.z;
                     const float4 r0 = sm.gd[stage][j][0], r1 = sm.gd[stage][j][1], r2 = sm.gd[stage][j][2];
-                    const float dx = x - r0.x, dy = y - r0.y, dz = z - r0.z;
-                    const float p2 = dx * fmaf(r1.x, dx, fmaf(r1.y, dy, r1.z * dz)) + dy * fmaf(r1.w, dy, r2.x * dz) +
-                                     dz * (r2.y * dz);
-                    const bool cc = in && p2 >= kLog2FloorC && p2 <= 0.0f;
-                    const float wt = cc ? r0.w * ex2_apx(p2) : 0.f;
-                    W += wt;
-                    V = fmaf(wt, r2.z, V);
-                    if (COUNT) {
-                        ncand += in ? 1 : 0;
-                        ncontrib += cc ? 1 : 0;
+#pragma unroll
+                    for (int k = 0; k < RPT; k++) {
+                        const float x = xr[k], y = yr[k], z = zr[k];
+                        const bool in =
+                            ing[k] && lo.x <= x && x <= hi.x && lo.y <= y && y <= hi.y && lo.z <= z && z <= hi.z;
+                        const float dx = x - r0.x, dy = y - r0.y, dz = z - r0.z;
+                        const float p2 = dx * fmaf(r1.x, dx, fmaf(r1.y, dy, r1.z * dz)) +
+                                         dy * fmaf(r1.w, dy, r2.x * dz) + dz * (r2.y * dz);
+                        const bool cc = in && p2 >= kLog2FloorC && p2 <= 0.0f;
+                        const float wt = cc ? r0.w * ex2_apx(p2) : 0.f;
+                        Wr[k] += wt;
+                        Vr[k] = fmaf(wt, r2.z, Vr[k]);
+                        if (COUNT) {
+                            ncand += in ? 1 : 0;
+                            ncontrib += cc ? 1 : 0;
+                        }
                     }
                 }
             }
@@ -597,18 +643,20 @@ __global__ void __launch_bounds__(kBlockRows + 32, TC ? kCtaMinBlocksTc : kCtaMi
             if (lane == 0) mbar_arrive(&sm.empty[stage]);
             n++;
         }
-        if (valid) {
-            const int orig = __float_as_int(spv.w);
-            float o, ww;
-            if (W <= kWeightCutoff) {
-                o = -1.0f;
-                ww = 0.0f;
-            } else {
-                o = V / W;
-                ww = W;
+#pragma unroll
+        for (int k = 0; k < RPT; k++) {
+            if (valid[k]) {
+                float o, ww;
+                if (Wr[k] <= kWeightCutoff) {
+                    o = -1.0f;
+                    ww = 0.0f;
+                } else {
+                    o = Vr[k] / Wr[k];
+                    ww = Wr[k];
+                }
+                out_cells[orig[k]] = o;
+                out_weights[orig[k]] = ww;
             }
-            out_cells[orig] = o;
-            out_weights[orig] = ww;
         }
         if (COUNT) {
             unsigned long long a = (unsigned long long)ncand, b = (unsigned long long)ncontrib;
@@ -643,11 +691,12 @@ cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32
 
 template <bool TC, bool COUNT>
 static cudaError_t launch_cta_impl(const CtaArgs& a, cudaStream_t st) {
+    constexpr int RPT = TC ? 1 : kSimtRowsPerThread;
     const size_t smem = sizeof(CtaSmem<TC>) + 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_forward_cta<TC, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_forward_cta<TC, COUNT, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    k_forward_cta<TC, COUNT><<<nblk128(a.S), kBlockRows + 32, smem, st>>>(a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes,
+    k_forward_cta<TC, COUNT, RPT><<<nblk128(a.S), (4 / RPT) * 32 + 32, smem, st>>>(a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes,
                                                                      a.recs, a.out_cells, a.out_weights, a.status,
                                                                      a.stats); gvc::note_launch();
     return cudaGetLastError();
