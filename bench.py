@@ -354,9 +354,27 @@ def run_ours(args):
         rast = R.GaussianRasterizer(settings)
         h2d = h_samples.numel() * 4 + sum(p.numel() * 4 for p in h_params)
 
-        def e2e_step():
-            s_d = h_samples.to(dev, non_blocking=True)
-            leaves = [p.to(dev, non_blocking=True).requires_grad_(True) for p in h_params]
+        # double-buffered uploads: the inputs of step k + 1 are copied on a second stream
+        # while step k computes (every step's copy is inside the timed region)
+        copy_stream = torch.cuda.Stream(dev)
+        hosts = [h_samples] + h_params
+        bufs = [[torch.empty(h.shape, dtype=h.dtype, device=dev) for h in hosts] for _ in range(2)]
+        ready = [torch.cuda.Event(), torch.cuda.Event()]
+
+        def issue_copy(b):
+            copy_stream.wait_stream(stream)  # the buffer's previous step has finished with it
+            with torch.cuda.stream(copy_stream):
+                for d_, h in zip(bufs[b], hosts):
+                    d_.copy_(h, non_blocking=True)
+                ready[b].record(copy_stream)
+
+        def e2e_step(k, n):
+            b = k % 2
+            stream.wait_event(ready[b])
+            if k + 1 < n:
+                issue_copy(1 - b)
+            s_d = bufs[b][0]
+            leaves = [p.detach().requires_grad_(True) for p in bufs[b][1:]]
             rast.build_bvh(s_d)
             cells, cw = rast(leaves[0], leaves[1], leaves[2], leaves[3], leaves[4])
             gt = target_field(s_d)
@@ -367,21 +385,25 @@ def run_ours(args):
                 gvc_dist.allreduce_grads([l.grad for l in leaves])
             return loss.item()
 
-        for _ in range(max(1, args.warmup)):
-            e2e_step()
+        def e2e_run(n):
+            issue_copy(0)
+            for k in range(n):
+                e2e_step(k, n)
+
+        e2e_run(max(1, args.warmup))
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         n_e2e = max(3, min(args.steps, 10))
         a0.record(stream)
-        for _ in range(n_e2e):
-            e2e_step()
+        e2e_run(n_e2e)
         a1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = gvc_dist.max_over_ranks(a0.elapsed_time(a1) / n_e2e, dev)
         e2e = {"value": e2e_ms, "unit": "ms/step", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4,
-               "steps": n_e2e, "path": "GaussianRasterizer (autograd) + masked L1 + loss.item()"}
+               "steps": n_e2e, "path": "GaussianRasterizer (autograd) + masked L1 + loss.item(); "
+                                         "pinned host inputs uploaded every step, double-buffered on a copy stream"}
 
     # the two evaluation paths side by side: full step time and forward outputs (kept on the
     # host for the FP64 comparison below)

@@ -56,73 +56,101 @@ __device__ __forceinline__ Box6 warp_box6(bool in, float x, float y, float z) {
     return b;
 }
 
-// Block-wide box of the rows with `in` set (all 128 threads call; result broadcast).
-__device__ Box6 block_box(bool in, float x, float y, float z, Box6* red) {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    Box6 b = warp_box6(in, x, y, z);
-    if (lane == 0) red[w] = b;
-    __syncthreads();
-    Box6 r = red[0];
-    for (int i = 1; i < 4; i++) {
-        r.lx = fminf(r.lx, red[i].lx);
-        r.ly = fminf(r.ly, red[i].ly);
-        r.lz = fminf(r.lz, red[i].lz);
-        r.hx = fmaxf(r.hx, red[i].hx);
-        r.hy = fmaxf(r.hy, red[i].hy);
-        r.hz = fmaxf(r.hz, red[i].hz);
-    }
-    __syncthreads();
-    return r;
-}
-
 __device__ __forceinline__ float hp6(const Box6& b) { return (b.hx - b.lx) + (b.hy - b.ly) + (b.hz - b.lz); }
 
-// Split row of [a, b) at the first differing key bit, or -1 (block-uniform).
-__device__ int block_split(int a, int b, const uint32_t* keys, uint32_t key, float x, float y, float z, Box6* red,
-                           int* ired) {
+// One warp per 128-row block; lane l holds rows 4l .. 4l + 3 (shuffles only, no block
+// barriers).  Box unions are min/max reductions, so the result does not depend on the
+// reduction order.
+__device__ __forceinline__ Box6 warp_reduce_box(Box6 b) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        b.lx = fminf(b.lx, __shfl_xor_sync(0xffffffffu, b.lx, off));
+        b.ly = fminf(b.ly, __shfl_xor_sync(0xffffffffu, b.ly, off));
+        b.lz = fminf(b.lz, __shfl_xor_sync(0xffffffffu, b.lz, off));
+        b.hx = fmaxf(b.hx, __shfl_xor_sync(0xffffffffu, b.hx, off));
+        b.hy = fmaxf(b.hy, __shfl_xor_sync(0xffffffffu, b.hy, off));
+        b.hz = fmaxf(b.hz, __shfl_xor_sync(0xffffffffu, b.hz, off));
+    }
+    return b;
+}
+
+// Box of the rows [a, b) (warp-collective).
+__device__ __forceinline__ Box6 rows_box(int a, int b, const float (&x)[4], const float (&y)[4], const float (&z)[4]) {
+    const int lane = threadIdx.x & 31;
+    Box6 r{INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int row = 4 * lane + k;
+        if (row >= a && row < b) {
+            r.lx = fminf(r.lx, x[k]);
+            r.ly = fminf(r.ly, y[k]);
+            r.lz = fminf(r.lz, z[k]);
+            r.hx = fmaxf(r.hx, x[k]);
+            r.hy = fmaxf(r.hy, y[k]);
+            r.hz = fmaxf(r.hz, z[k]);
+        }
+    }
+    return warp_reduce_box(r);
+}
+
+// Split row of [a, b) or -1 (warp-uniform): at the first Morton bit where the range's
+// first and last keys differ, taken when both halves' boxes have at most half the
+// half-perimeter of the whole.
+__device__ int rows_split(int a, int b, const uint32_t* keys, const uint32_t (&key)[4], const float (&x)[4],
+                          const float (&y)[4], const float (&z)[4]) {
     if (b - a < 2) return -1;
     const uint32_t ka = keys[a], kb = keys[b - 1];
     if (ka == kb) return -1;
     const int bit = 31 - __clz(ka ^ kb);
-    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
-    const bool in = t >= a && t < b;
-    const uint32_t hi = __ballot_sync(0xffffffffu, in && ((key >> bit) & 1u));
-    if (lane == 0) ired[w] = hi ? 32 * w + __ffs(hi) - 1 : kBlockRows;
-    __syncthreads();
-    const int m = min(min(ired[0], ired[1]), min(ired[2], ired[3]));
-    __syncthreads();
-    const Box6 B = block_box(in, x, y, z, red);
-    const Box6 B1 = block_box(in && t < m, x, y, z, red);
-    const Box6 B2 = block_box(in && t >= m, x, y, z, red);
+    const int lane = threadIdx.x & 31;
+    int first = kBlockRows;  // keys are sorted: the rows with the bit set are a suffix of [a, b)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int row = 4 * lane + k;
+        if (row >= a && row < b && ((key[k] >> bit) & 1u)) first = min(first, row);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, off));
+    const int m = first;
+    const Box6 B = rows_box(a, b, x, y, z);
+    const Box6 B1 = rows_box(a, m, x, y, z);
+    const Box6 B2 = rows_box(m, b, x, y, z);
     return fmaxf(hp6(B1), hp6(B2)) <= 0.5f * hp6(B) ? m : -1;
 }
 
+constexpr int kBlocksPerCta = 8;  // 128-row blocks (warps) per CTA of k_sample_blocks
+
 // bdesc[blk] = (starts of groups 1..7 as bytes, 128 if unused; byte 7 = group count);
-// bboxes[blk * 8 + g] = (lo, hi) of group g (empty box if unused).
-__global__ void __launch_bounds__(kBlockRows) k_sample_blocks(const float4* __restrict__ s_sorted,
-                                                              const uint32_t* __restrict__ skeys, int64_t S,
-                                                              int64_t n_blocks, uint2* __restrict__ bdesc,
-                                                              float4* __restrict__ bboxes) {
-    __shared__ uint32_t keys[kBlockRows];
-    __shared__ Box6 red[4];
-    __shared__ int ired[4];
-    const int64_t blk = blockIdx.x;
-    const int t = threadIdx.x;
-    const int64_t row = blk * kBlockRows + t;
-    const bool valid = row < S;
-    float x = NAN, y = NAN, z = NAN;
-    uint32_t key = 0xffffffffu;
-    if (valid) {
-        const float4 p = s_sorted[row];
-        x = p.x;
-        y = p.y;
-        z = p.z;
-        key = skeys[row];
+// bboxes[blk * 8 + g] = (lo, hi) of group g (empty box if unused).  The range [0, nvalid)
+// is split three times (every range of a level in order), giving at most 8 groups.
+__global__ void __launch_bounds__(32 * kBlocksPerCta) k_sample_blocks(const float4* __restrict__ s_sorted,
+                                                                      const uint32_t* __restrict__ skeys, int64_t S,
+                                                                      int64_t n_blocks, uint2* __restrict__ bdesc,
+                                                                      float4* __restrict__ bboxes) {
+    __shared__ uint32_t s_keys[kBlocksPerCta][kBlockRows];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t blk = (int64_t)blockIdx.x * kBlocksPerCta + warp;
+    if (blk >= n_blocks) return;
+    uint32_t* keys = s_keys[warp];
+    float x[4], y[4], z[4];
+    uint32_t key[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int64_t row = blk * kBlockRows + 4 * lane + k;
+        x[k] = y[k] = z[k] = NAN;
+        key[k] = 0xffffffffu;
+        if (row < S) {
+            const float4 p = s_sorted[row];
+            x[k] = p.x;
+            y[k] = p.y;
+            z[k] = p.z;
+            key[k] = skeys[row];
+        }
+        keys[4 * lane + k] = key[k];
     }
-    keys[t] = key;
+    __syncwarp();
     const int64_t rem = S - blk * kBlockRows;
     const int nvalid = rem < kBlockRows ? (int)rem : kBlockRows;
-    __syncthreads();
     int ra[kBlockGroups], rb[kBlockGroups];
     int nr = 1;
     ra[0] = 0;
@@ -131,7 +159,7 @@ __global__ void __launch_bounds__(kBlockRows) k_sample_blocks(const float4* __re
         int na[kBlockGroups], nbb[kBlockGroups];
         int nn = 0;
         for (int i = 0; i < nr; i++) {
-            const int m = block_split(ra[i], rb[i], keys, key, x, y, z, red, ired);
+            const int m = rows_split(ra[i], rb[i], keys, key, x, y, z);
             if (m >= 0) {
                 na[nn] = ra[i];
                 nbb[nn++] = m;
@@ -151,18 +179,14 @@ __global__ void __launch_bounds__(kBlockRows) k_sample_blocks(const float4* __re
     uint32_t starts[kBlockGroups];
     for (int g = 0; g < kBlockGroups; g++) starts[g] = g < nr ? (uint32_t)ra[g] : (uint32_t)kBlockRows;
     for (int g = 0; g < kBlockGroups; g++) {
-        Box6 B;
-        if (g < nr) {
-            B = block_box(valid && t >= ra[g] && t < rb[g], x, y, z, red);
-        } else {
-            B = Box6{INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-        }
-        if (t == 0) {
+        Box6 B{INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+        if (g < nr) B = rows_box(ra[g], rb[g], x, y, z);
+        if (lane == 0) {
             bboxes[2 * (blk * kBlockGroups + g)] = make_float4(B.lx, B.ly, B.lz, 0.f);
             bboxes[2 * (blk * kBlockGroups + g) + 1] = make_float4(B.hx, B.hy, B.hz, 0.f);
         }
     }
-    if (t == 0) {
+    if (lane == 0) {
         uint2 d;
         d.x = starts[1] | (starts[2] << 8) | (starts[3] << 16) | (starts[4] << 24);
         d.y = starts[5] | (starts[6] << 8) | (starts[7] << 16) | ((uint32_t)nr << 24);
@@ -685,7 +709,9 @@ cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32
                                  float4* bboxes, cudaStream_t st) {
     if (S <= 0) return cudaSuccess;
     const int64_t nb = (S + kBlockRows - 1) / kBlockRows;
-    k_sample_blocks<<<(unsigned)nb, kBlockRows, 0, st>>>(s_sorted, skeys, S, nb, bdesc, bboxes); gvc::note_launch();
+    k_sample_blocks<<<(unsigned)((nb + kBlocksPerCta - 1) / kBlocksPerCta), 32 * kBlocksPerCta, 0, st>>>(
+        s_sorted, skeys, S, nb, bdesc, bboxes);
+    gvc::note_launch();
     return cudaGetLastError();
 }
 
