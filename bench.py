@@ -378,8 +378,9 @@ def run_ours(args):
             rast.build_bvh(s_d)
             cells, cw = rast(leaves[0], leaves[1], leaves[2], leaves[3], leaves[4])
             gt = target_field(s_d)
-            mask = (cells != -1) & (gt != -1)
-            loss = torch.abs(cells[mask] - gt[mask]).mean()
+            # masked mean without boolean indexing (no device-to-host size query)
+            mask = ((cells != -1) & (gt != -1)).float()
+            loss = (torch.abs(cells - gt) * mask).sum() / mask.sum().clamp_min(1.0)
             loss.backward()
             if world > 1:
                 gvc_dist.allreduce_grads([l.grad for l in leaves])

@@ -209,6 +209,10 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint32_t* __restrict__
                                                     const uint32_t* __restrict__ totals) {
     __shared__ uint32_t wcnt[kRsWarps][256];
     __shared__ uint32_t dbase[256];
+    __shared__ uint32_t bstart[256];
+    __shared__ uint32_t wsum[kRsWarps];
+    __shared__ uint32_t skey[kRsTile];
+    __shared__ int32_t sval[kRsTile];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int shift = 8 * pass;
     for (int t = threadIdx.x; t < kRsWarps * 256; t += blockDim.x) (&wcnt[0][0])[t] = 0;
@@ -251,27 +255,52 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint32_t* __restrict__
         rreg[it] = valid ? (((pre + rank) << 8) | d) : 0xffffffffu;
     }
     __syncthreads();
-    // exclusive prefix over warps for each digit
+    // exclusive prefix over warps for each digit; run = this block's count of digit d
+    uint32_t run = 0;
     {
-        int d = threadIdx.x;  // 256 threads == 256 digits
-        uint32_t run = 0;
+        const int d = threadIdx.x;  // 256 threads == 256 digits
 #pragma unroll
         for (int w = 0; w < kRsWarps; w++) {
-            uint32_t t = wcnt[w][d];
+            const uint32_t t = wcnt[w][d];
             wcnt[w][d] = run;
             run += t;
         }
     }
+    // block-local start of each digit: exclusive scan of the 256 counts
+    {
+        uint32_t incl = run;
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += t;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t wbase = 0;
+        for (int w = 0; w < warp; w++) wbase += wsum[w];
+        bstart[threadIdx.x] = wbase + incl - run;
+    }
     __syncthreads();
+    // place every key at its block-local sorted position, then write the block out in that
+    // order: consecutive threads write consecutive addresses of each digit's run
 #pragma unroll
     for (int it = 0; it < kRsIters; it++) {
-        uint32_t r = rreg[it];
+        const uint32_t r = rreg[it];
         if (r != 0xffffffffu) {
-            uint32_t d = r & 255u;
-            uint32_t pos = dbase[d] + wcnt[warp][d] + (r >> 8);
-            keys_out[pos] = kreg[it];
-            vals_out[pos] = vreg[it];
+            const uint32_t d = r & 255u;
+            const uint32_t sp = bstart[d] + wcnt[warp][d] + (r >> 8);
+            skey[sp] = kreg[it];
+            sval[sp] = vreg[it];
         }
+    }
+    __syncthreads();
+    const int64_t rem = n - (int64_t)blockIdx.x * kRsTile;
+    const int cnt = rem < kRsTile ? (int)rem : kRsTile;
+    for (int sp = threadIdx.x; sp < cnt; sp += blockDim.x) {
+        const uint32_t key = skey[sp];
+        const uint32_t d = (key >> shift) & 255u;
+        const uint32_t pos = dbase[d] + ((uint32_t)sp - bstart[d]);
+        keys_out[pos] = key;
+        vals_out[pos] = sval[sp];
     }
 }
 
