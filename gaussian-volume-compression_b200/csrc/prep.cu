@@ -200,6 +200,11 @@ __device__ __forceinline__ float half_perimeter(const WBox& b) {
     return (b.hx - b.lx) + (b.hy - b.ly) + (b.hz - b.lz);
 }
 
+// A lane group is split when both halves' boxes have at most this fraction of the whole's
+// half-perimeter (0.65 measured best for the backward's candidate rows: 0.5 gathers 9.4e9
+// rows at 2M x 16M, 0.65 8.5e9; from 0.8 on the extra leaves cost more than they save).
+constexpr float kTileSplitRatio = 0.65f;
+
 // Split lane of group [a, b), or -1 (warp-uniform).
 __device__ int try_split(int a, int b, uint32_t key, int lane, float x, float y, float z) {
     if (b - a < 2) return -1;
@@ -213,7 +218,7 @@ __device__ int try_split(int a, int b, uint32_t key, int lane, float x, float y,
     const WBox B1 = warp_box(in && lane < m, x, y, z);
     const WBox B2 = warp_box(in && lane >= m, x, y, z);
     const float h = half_perimeter(B);
-    return fmaxf(half_perimeter(B1), half_perimeter(B2)) <= 0.5f * h ? m : -1;
+    return fmaxf(half_perimeter(B1), half_perimeter(B2)) <= kTileSplitRatio * h ? m : -1;
 }
 
 __global__ void __launch_bounds__(256) k_sample_tiles(int64_t S, int64_t n_tiles, const float* __restrict__ samples,
