@@ -67,6 +67,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile", action="store_true", help="minimal run for ncu (no e2e, no CPU baseline)")
+    p.add_argument("--mesh", action="store_true",
+                   help="also time the mesh samplers (128^3 jittered hex grid split into 12.6M tetrahedra, "
+                        "256^3 uniform grid, 8M points each) and add a mesh_sampler object")
     return p.parse_args()
 
 
@@ -235,6 +238,75 @@ def run_reference(args):
             "note": "the reference CUDA extension is not buildable (cuBQL, glm and Viskores sources absent); "
                     "this arm is the reference formula restated in C (oracle/gvc_oracle.c)"}
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------
+# Mesh samplers (sample_meshu / sample_mesh): device-resident inputs, CUDA-event timing
+# ----------------------------------------------------------------------------------------
+def mesh_bench(dev, steps, warmup, with_cpu):
+    import ctypes
+    import torch
+    import gvc_native
+    import gvc_workloads as wl
+    rng = np.random.default_rng(11)
+    n_pts = 8_000_000
+    res = {}
+    ctx = gvc_native.Context()
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ctx.sync_status(stream.cuda_stream)
+        return e0.elapsed_time(e1) / steps
+
+    # tetrahedra: 128^3 jittered hex grid, 6 tets per hex (12,582,912 cells), 8M points
+    pts, tets = wl.jittered_tet_mesh(n=128, seed=7)
+    vals = wl.blob_field(pts).astype(np.float64)
+    q = rng.random((n_pts, 3), dtype=np.float32)
+    d_pts, d_tets, d_vals, d_q = T(pts), T(tets.astype(np.int32)), T(vals), T(q)
+    d_out = torch.empty(n_pts, dtype=torch.float64, device=dev)
+    d_cell = torch.empty(n_pts, dtype=torch.int64, device=dev)
+    ms = timed(lambda: ctx.call("gvc_sample_tets", pts.shape[0], gvc_native.ptr(d_pts), tets.shape[0],
+                                gvc_native.ptr(d_tets), gvc_native.ptr(d_vals), n_pts, gvc_native.ptr(d_q),
+                                gvc_native.ptr(d_out), gvc_native.ptr(d_cell), sp))
+    tet = {"cells": int(tets.shape[0]), "points": n_pts, "ms_per_call": ms, "points_per_s": n_pts / (ms * 1e-3),
+           "includes": "cell LBVH build (keys, sort, Karras, refit) + point sort + locate + interpolate",
+           "found": float((d_cell >= 0).float().mean().item())}
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        sub = q[:1_000_000]
+        t0 = time.perf_counter()
+        oracle.sample_tets(pts, tets, vals, sub)
+        t = time.perf_counter() - t0
+        tet["cpu_oracle"] = {"points_per_s": sub.shape[0] / t, "cores": os.cpu_count() or 1,
+                             "sample": "oracle (C, OpenMP, uniform grid locator) on 1M of the points, "
+                                       "locator build included (%.2f s)" % t}
+    res["tets"] = tet
+    del d_pts, d_tets, d_vals
+    # uniform grid: 256^3 float32 point values, trilinear, 8M points
+    dims = np.array([256, 256, 256], np.int64)
+    origin = np.zeros(3, np.float32)
+    spacing = np.full(3, 1.0 / 255, np.float32)
+    gvals = rng.random(int(dims.prod()), dtype=np.float32)
+    d_g = T(gvals.view(np.uint8))
+    d_o = torch.empty(n_pts * 4, dtype=torch.uint8, device=dev)
+    ms = timed(lambda: ctx.call("gvc_sample_uniform", gvc_native.ptr(dims), gvc_native.ptr(origin),
+                                gvc_native.ptr(spacing), gvc_native.ptr(d_g), gvc_native.DTYPE_CODES["float32"],
+                                n_pts, gvc_native.ptr(d_q), gvc_native.ptr(d_o), sp))
+    res["uniform"] = {"dims": [256, 256, 256], "dtype": "float32", "points": n_pts, "ms_per_call": ms,
+                      "points_per_s": n_pts / (ms * 1e-3)}
+    return res
 
 
 # ----------------------------------------------------------------------------------------
@@ -456,6 +528,8 @@ def run_ours(args):
                            else "single GPU"},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e, "tc_vs_plain": tc_vs_plain,
                 "gpu_launches": int(launches), "gpu_launches_per_step": launches / args.steps}
+        if args.mesh and world == 1:
+            line["mesh_sampler"] = mesh_bench(dev, 5, 2, not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
