@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Benchmark of the Gaussian-mixture volume training step on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config large|medium|small]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config large|medium|small|slice|tiny] [--eval-path plain|tensor_core|plain_tile] [--mesh]
 
 Metric: fwd+bwd ms per step at 2M Gaussians x 16M points (the "large evaluation"
 configuration: clustered means, half the samples near Gaussian means).  One step is what
@@ -37,6 +38,7 @@ CONFIGS = {
     "medium": (200_000, 4_000_000, "scaled large evaluation: 200k clustered Gaussians x 4M points"),
     "small": (200_000, 2_000_000, "profiling case: 200k clustered Gaussians x 2M points"),
     "slice": (2_000_000, 4_000_000, "profiling case with the large evaluation's Gaussians: 2M clustered Gaussians x 4M points"),
+    "tiny": (4_096, 262_144, "CPU-runnable case: 4096 clustered Gaussians x 64^3 points"),
 }
 METRIC = "fwd+bwd ms/step (2M Gaussians×16M pts), TC vs plain FP32 at stated FP64 err"
 # Algorithmic FP32 work per pair (FORWARD forward.cu:224-256, BACKWARD backward.cu:252-298):
@@ -170,6 +172,12 @@ def cpu_baseline(means, scales, rots, values, weights, samples, sizes=(250_000, 
     import oracle
     oracle.lib()
     threads = os.cpu_count() or 1
+    S = samples.shape[0]
+    if S <= sizes[1]:
+        t = cpu_step_time(means, scales, rots, values, weights, samples, S)
+        return {"value": t * 1e3, "unit": "ms/step", "cores": threads, "kind": "port",
+                "sample": "oracle fwd+bwd (C, OpenMP %d threads) on the full step: all %d points and %d Gaussians"
+                          % (threads, S, means.shape[0]), "extrapolated": False}
     t = [cpu_step_time(means, scales, rots, values, weights, samples, n) for n in sizes]
     slope = (t[1] - t[0]) / (sizes[1] - sizes[0])
     fixed = max(t[0] - slope * sizes[0], 0.0)
@@ -219,7 +227,7 @@ def run_reference(args):
     oracle.lib()
     threads = os.cpu_count() or 1
     S = samples.shape[0]
-    n_a, n_b = 125_000, 500_000
+    n_a, n_b = min(125_000, S // 4), min(500_000, S)
     t_a = cpu_step_time(means, scales, rots, values, weights, samples, n_a)
     for _ in range(max(args.warmup - 1, 0)):
         cpu_step_time(means, scales, rots, values, weights, samples, n_b)

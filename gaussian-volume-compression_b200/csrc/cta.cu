@@ -263,7 +263,10 @@ __global__ void __launch_bounds__(128) k_tc_gemm_test(const __nv_bfloat16* __res
 //   full[s]  completes when the producer has staged s (arrive) and its MMAs are done (commit);
 //   empty[s] completes when the four consumer warps have released s.
 // ---------------------------------------------------------------------------------------
-constexpr int kStages = 4;
+// Batches in flight: 4 for the SIMT variant; 2 for the tensor-core variant, whose smaller
+// operand ring lets 6 CTAs share an SM (24.6 ms instead of 26.2 ms at 2M x 16M).
+template <bool TC>
+constexpr int kStagesOf = TC ? 2 : 4;
 constexpr int kBatch = 32;  // Gaussians per MMA batch (N)
 
 __device__ __forceinline__ bool overlap6(const Box6& b, float4 lo, float4 hi) {
@@ -275,20 +278,20 @@ __device__ __forceinline__ bool overlap6(const Box6& b, float4 lo, float4 hi) {
 template <bool TC>
 struct CtaTcOperands {
     unsigned char A[3][kBlockRows * 32];       // phi(u), three bf16 parts
-    unsigned char B[kStages][3][kBatch * 32];  // beta, three bf16 parts, per stage
+    unsigned char B[kStagesOf<TC>][3][kBatch * 32];  // beta, three bf16 parts, per stage
 };
 template <>
 struct CtaTcOperands<false> {};
 
 template <bool TC>
 struct CtaSmem : CtaTcOperands<TC> {
-    float4 gd[kStages][kBatch][5];                 // (mu, w), C'(0..3), (C'4, C'5, v, -), lo, hi
-    uint8_t colmask[kStages][kBatch];              // bits 0..3: column overlaps warp w; bit 4: SIMT fallback
-    int2 desc[kStages];                            // (number of columns or -1 at the end, group)
+    float4 gd[kStagesOf<TC>][kBatch][5];                 // (mu, w), C'(0..3), (C'4, C'5, v, -), lo, hi
+    uint8_t colmask[kStagesOf<TC>][kBatch];              // bits 0..3: column overlaps warp w; bit 4: SIMT fallback
+    int2 desc[kStagesOf<TC>];                            // (number of columns or -1 at the end, group)
     Box6 wb[4];                                    // boxes of the current group's rows of each consumer warp
     int stack[kStackCap];
     int cand[kCandCap];
-    uint64_t full[kStages], empty[kStages];
+    uint64_t full[kStagesOf<TC>], empty[kStagesOf<TC>];
     uint32_t tmem_base;
 };
 
@@ -307,6 +310,7 @@ __device__ __forceinline__ void cp_async_wait() {
 // the next batch's copies are in flight.
 template <bool TC, bool COUNT, int NCW>
 struct Producer {
+    static constexpr int kStages = kStagesOf<TC>;
     CtaSmem<TC>& sm;
     const GaussRec* __restrict__ recs;
     int* status;
@@ -442,10 +446,10 @@ struct Producer {
 };
 
 // Resident CTAs per SM requested from the register allocator.  The tensor-core variant
-// (4 consumer warps, one row per thread) runs 5 (its shared memory allows 6); the SIMT
+// (4 consumer warps, one row per thread) runs 6; the SIMT
 // variant with one row per thread fits 8 (40 warps), with two rows per thread 16
 // (48 warps, 40 registers).
-constexpr int kCtaMinBlocksTc = 5;
+constexpr int kCtaMinBlocksTc = 6;
 constexpr int kCtaMinBlocksSimt1 = 8;
 constexpr int kCtaMinBlocksSimt2 = 16;
 // Rows per consumer thread of the SIMT variant: each staged record (80 bytes broadcast to
@@ -462,6 +466,7 @@ __global__ void __launch_bounds__((4 / RPT) * 32 + 32,
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     CtaSmem<TC>& sm = *reinterpret_cast<CtaSmem<TC>*>(smem_raw);
     static_assert(!TC || RPT == 1, "the tensor-core variant owns one row (TMEM lane) per thread");
+    constexpr int kStages = kStagesOf<TC>;
     constexpr int NCW = 4 / RPT;  // consumer warps; warp NCW is the producer
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int64_t blk = blockIdx.x;
