@@ -648,12 +648,21 @@ __global__ void __launch_bounds__((4 / RPT) * 32 + 32,
                     const int j = __ffs(mm) - 1;
                     mm &= mm - 1;
                     const float4 lo = sm.gd[stage][j][3], hi = sm.gd[stage][j][4];
+                    bool inr[RPT];
+                    bool anyin = false;
+#pragma unroll
+                    for (int k = 0; k < RPT; k++) {
+                        const float x = xr[k], y = yr[k], z = zr[k];
+                        inr[k] = ing[k] && lo.x <= x && x <= hi.x && lo.y <= y && y <= hi.y && lo.z <= z && z <= hi.z;
+                        anyin |= inr[k];
+                    }
+                    // the column's box overlaps the warp's rows, but often no row lies inside it
+                    if (!__any_sync(0xffffffffu, anyin)) continue;
                     const float4 r0 = sm.gd[stage][j][0], r1 = sm.gd[stage][j][1], r2 = sm.gd[stage][j][2];
 #pragma unroll
                     for (int k = 0; k < RPT; k++) {
                         const float x = xr[k], y = yr[k], z = zr[k];
-                        const bool in =
-                            ing[k] && lo.x <= x && x <= hi.x && lo.y <= y && y <= hi.y && lo.z <= z && z <= hi.z;
+                        const bool in = inr[k];
                         const float dx = x - r0.x, dy = y - r0.y, dz = z - r0.z;
                         const float p2 = dx * fmaf(r1.x, dx, fmaf(r1.y, dy, r1.z * dz)) +
                                          dy * fmaf(r1.w, dy, r2.x * dz) + dz * (r2.y * dz);
