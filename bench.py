@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="large", choices=list(CONFIGS))
-    p.add_argument("--bwd-mode", default="auto", choices=["auto", "deterministic", "atomic"])
+    p.add_argument("--bwd-mode", default="auto", choices=["auto", "deterministic", "atomic", "tensor_core"])
     p.add_argument("--eval-path", default="plain", choices=["plain", "tensor_core", "plain_tile"])
     p.add_argument("--use-gaussian-bvh", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -398,7 +398,8 @@ def run_ours(args):
     t_fwd = kt["fwd_kernel_ms"] / max(kt["fwd_kernel_calls"], 1)
     t_bwd = kt["bwd_kernel_ms"] / max(kt["bwd_kernel_calls"], 1)
     hbm, bf16, bf16s, src = measured_peaks()
-    bwd_kernel = "k_backward_cta" if args.eval_path == "tensor_core" and args.bwd_mode != "deterministic" else (
+    bwd_kernel = "k_backward_cta" if args.bwd_mode == "tensor_core" or (
+        args.eval_path == "tensor_core" and args.bwd_mode == "auto") else (
         "k_backward_tiles" if args.bwd_mode == "atomic" or (args.bwd_mode == "auto" and ugb) else "k_backward_gauss")
     fwd_kernel = "k_forward" if args.eval_path == "plain_tile" else "k_forward_cta"
     if t_bwd >= t_fwd:
@@ -489,9 +490,14 @@ def run_ours(args):
     # the two evaluation paths side by side: full step time and forward outputs (kept on the
     # host for the FP64 comparison below)
     paths = {}
+    paths_extra = {}
     if not args.profile:
-        for path in ("plain", "tensor_core"):
+        # (forward path, backward mode): FP32 throughout, tensor cores throughout, and the FP32
+        # forward with the tensor-core backward reduction
+        for name, path, bmode in (("plain", "plain", "auto"), ("tensor_core", "tensor_core", "auto"),
+                                  ("plain_fwd_tc_bwd", "plain", "tensor_core")):
             _C.set_eval_path(path)
+            _C.set_backward_mode(bmode)
             for _ in range(2):
                 step()
             torch.cuda.synchronize()
@@ -504,12 +510,16 @@ def run_ours(args):
             b1.record(stream)
             torch.cuda.synchronize()
             pm = gvc_dist.max_over_ranks(b0.elapsed_time(b1) / args.steps, dev)
+            if name == "plain_fwd_tc_bwd":
+                paths_extra = {"plain_fwd_tc_bwd_ms_per_step": pm}
+                continue
             _C.build_bvh(d_samples, False, ugb)
             o, ow, cn = _C.rasterize_gaussians(d_means, d_scales, d_rots, d_values, d_weights, 1.0, *bounds, -1.0,
                                                ugb, False)
-            paths[path] = {"ms_per_step": pm, "out": o.cpu().numpy(), "outw": ow.cpu().numpy(),
+            paths[name] = {"ms_per_step": pm, "out": o.cpu().numpy(), "outw": ow.cpu().numpy(),
                            "conics": cn.cpu().numpy().reshape(-1, 6)}
         _C.set_eval_path(args.eval_path)
+        _C.set_backward_mode(args.bwd_mode)
         _C.check_status()
 
     cpu = None
@@ -523,6 +533,7 @@ def run_ours(args):
                        "tensor_core_ms_per_step": paths["tensor_core"]["ms_per_step"],
                        "speedup_tc_over_plain": paths["plain"]["ms_per_step"] / paths["tensor_core"]["ms_per_step"],
                        "fp64_error": fp64}
+        tc_vs_plain.update(paths_extra)
 
     if rank == 0:
         line = {"metric": METRIC, "value": ms, "unit": "ms/step", "n_gpus": world, "steps": args.steps,

@@ -185,8 +185,9 @@ def set_cov_grad_mode(mode, device=None):
 
 
 def set_backward_mode(mode, device=None):
-    """'auto' (follow use_gaussian_bvh), 'deterministic' or 'atomic'."""
-    set_option(_n.OPT_BWD_MODE, {"auto": 0, "deterministic": 1, "atomic": 2}[mode], device)
+    """'auto' (follow use_gaussian_bvh; the tensor-core reduction on the tensor-core eval
+    path), 'deterministic', 'atomic' (sample-tile traversal) or 'tensor_core'."""
+    set_option(_n.OPT_BWD_MODE, {"auto": 0, "deterministic": 1, "atomic": 2, "tensor_core": 3}[mode], device)
 
 
 def set_eval_path(path, device=None):

@@ -290,6 +290,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                         break;
                     }
                 }
+                // branch-free over the 16 rows: independent chains the scheduler can interleave
+                // (a per-row warp vote to skip missing rows measured 15 % slower)
                 float e[16];
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
@@ -297,19 +299,16 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                     const float4 p = sm.rows[r];
                     const bool in = r >= ra && r < rb && g.lx <= p.x && p.x <= g.hx && g.ly <= p.y && p.y <= g.hy &&
                                     g.lz <= p.z && p.z <= g.hz;
-                    e[k] = 0.f;
-                    if (__any_sync(0xffffffffu, in)) {
-                        const float dx = p.x - g.mx, dy = p.y - g.my, dz = p.z - g.mz;
-                        const float p2 = dx * fmaf(g.q0, dx, fmaf(g.q1, dy, g.q2 * dz)) +
-                                         dy * fmaf(g.q3, dy, g.q4 * dz) + dz * (g.q5 * dz);
-                        const bool c = in && p2 >= kLog2Floor && p2 <= 0.0f;
-                        e[k] = c ? ex2_approx(p2) : 0.f;
-                        anyc |= c;
-                        if (COUNT) {
-                            ncand += in ? 1 : 0;
-                            ncontrib += (c && p.w != 0.f) ? 1 : 0;
-                            nlane += 32;
-                        }
+                    const float dx = p.x - g.mx, dy = p.y - g.my, dz = p.z - g.mz;
+                    const float p2 = dx * fmaf(g.q0, dx, fmaf(g.q1, dy, g.q2 * dz)) +
+                                     dy * fmaf(g.q3, dy, g.q4 * dz) + dz * (g.q5 * dz);
+                    const bool c = in && p2 >= kLog2Floor && p2 <= 0.0f;
+                    e[k] = c ? ex2_approx(p2) : 0.f;
+                    anyc |= c;
+                    if (COUNT) {
+                        ncand += in ? 1 : 0;
+                        ncontrib += (c && p.w != 0.f) ? 1 : 0;
+                        nlane += 32;
                     }
                 }
                 tc_fence_after();

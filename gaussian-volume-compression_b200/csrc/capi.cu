@@ -207,7 +207,7 @@ int gvc_set_option(gvc_ctx* ctx, int option, int value) {
             ctx->cov_grad_mode = value;
             return GVC_OK;
         case GVC_OPT_BWD_MODE:
-            if (value < 0 || value > 2) return fail(ctx, GVC_ERR_ARG, "bwd_mode must be 0, 1 or 2");
+            if (value < 0 || value > 3) return fail(ctx, GVC_ERR_ARG, "bwd_mode must be 0, 1, 2 or 3");
             ctx->bwd_mode = value;
             return GVC_OK;
         case GVC_OPT_EVAL_PATH:
@@ -408,10 +408,9 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
              "preprocess");
     GVC_CUDA(sc->gacc.ensure(sizeof(float) * 16 * P), "alloc gacc");
     float* gacc = sc->gacc.as<float>();
+    // mode 3, or the tensor-core path in auto mode: reduction over samples on tcgen05
+    const bool tc_bwd = ctx->bwd_mode == 3 || (ctx->bwd_mode == 0 && ctx->eval_path == 1);
     const bool atomic_mode = ctx->bwd_mode == 2 || (ctx->bwd_mode == 0 && use_gaussian_bvh);
-    // the tensor-core path reduces over samples on tcgen05 (atomic accumulation) unless the
-    // deterministic reduction is forced
-    const bool tc_bwd = ctx->eval_path == 1 && ctx->bwd_mode != 1;
     const bool have_order = ctx->gauss_ready && ctx->P == P;
     if (ctx->n_tiles == 0) {
         GVC_CUDA(cudaMemsetAsync(gacc, 0, sizeof(float) * 16 * P, st), "zero gacc");

@@ -44,11 +44,15 @@ typedef enum {
                                    (deterministic, no atomics; mirrors backward.cu:127-337),
                                    use_gaussian_bvh != 0 -> sample-tile traversal with warp
                                    pre-reduction + FP32 atomics (mirrors backward.cu:339-559);
-                               1 = always deterministic, 2 = always atomic                */
+                                   (with GVC_OPT_EVAL_PATH = 1: the tensor-core reduction, 3);
+                               1 = always deterministic, 2 = always sample-tile atomic,
+                               3 = tensor core: per 128-sample block, the per-Gaussian sums
+                                   over samples as a tcgen05 BF16 3-way split GEMM in TMEM,
+                                   FP32 atomics (not bitwise reproducible)                  */
     GVC_OPT_EVAL_PATH = 3,  /* forward evaluation kernel (all compute the same field):
                                0 = FP32 exponent, one CTA per 128-sample block: a producer warp
-                                   walks the Gaussian LBVH and stages batches, four consumer
-                                   warps evaluate (default, fastest),
+                                   walks the Gaussian LBVH and stages batches, two consumer
+                                   warps evaluate two samples per thread (default, fastest),
                                1 = tensor-core exponent: the same pipeline with the power as a
                                    tcgen05 BF16 3-way split MMA into TMEM,
                                2 = FP32 exponent, one warp per 32-sample tile               */

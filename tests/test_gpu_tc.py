@@ -110,16 +110,18 @@ def run_backward_path(dev, case, gout, gw, path, mode="auto"):
         _C.set_eval_path("plain")
 
 
-@pytest.mark.parametrize("gw_scale", [0.0, 1.0])
-def test_tensor_core_backward_matches_oracle(cuda, orc, case, gw_scale):
+@pytest.mark.parametrize("gw_scale,path,mode", [(0.0, "tensor_core", "auto"), (1.0, "tensor_core", "auto"),
+                                                (1.0, "plain", "tensor_core")])
+def test_tensor_core_backward_matches_oracle(cuda, orc, case, gw_scale, path, mode):
     """The tensor-core backward (per-Gaussian reduction over samples as a split-BF16 GEMM
-    in tensor memory) against the oracle's FP64 adjoint at the forward's own outputs."""
+    in tensor memory) against the oracle's FP64 adjoint at the forward's own outputs, on
+    the tensor-core path and selected explicitly after the FP32 forward."""
     from test_gpu_rasterizer import assert_grads_close, oracle_backward
     S = case[-1].shape[0]
     rng = np.random.default_rng(31)
     gout = rng.normal(size=S).astype(np.float32)
     gw = (gw_scale * rng.normal(size=S)).astype(np.float32)
-    got, out, outw, conics = run_backward_path(cuda, case, gout, gw, "tensor_core")
+    got, out, outw, conics = run_backward_path(cuda, case, gout, gw, path, mode)
     ref = oracle_backward(orc, case, out, outw, conics, gout, gw)
     for k, name in enumerate(("means", "scales", "rots", "values", "weights")):
         print("%s: max err / max |ref| = %.2e" % (name, np.abs(got[k] - ref[k]).max() / np.abs(ref[k]).max()))
