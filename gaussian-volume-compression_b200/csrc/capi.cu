@@ -185,7 +185,7 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
                           &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds};
         for (DevBuf* b : bufs) b->release();
     }
-    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
+    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->blk_desc_b, &c->blk_boxes_b, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
                       &c->m_out_sorted, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
     for (DevBuf* b : bufs) b->release();
     if (c->d_status) cudaFree(c->d_status);
@@ -270,6 +270,7 @@ int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int 
     ctx->S = S;
     ctx->n_tiles = (S + kTile - 1) / kTile;
     ctx->samples_ready = false;
+    ctx->blk_b_ready = false;
     if (S > 0) {
         GVC_CUDA(morton_sort_points(ctx->s_sort, S, samples, st), "sample sort");
         const int64_t slots = ctx->n_tiles * kTile;
@@ -289,7 +290,7 @@ int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int 
         GVC_CUDA(ctx->blk_desc.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc");
         GVC_CUDA(ctx->blk_boxes.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes");
         GVC_CUDA(launch_sample_blocks(S, ctx->s_sorted.as<float4>(), ctx->s_sort.keys.as<uint32_t>(),
-                                      ctx->blk_desc.as<uint2>(), ctx->blk_boxes.as<float4>(), st),
+                                      ctx->blk_desc.as<uint2>(), ctx->blk_boxes.as<float4>(), kBlockSplitForward, st),
                  "sample blocks");
     }
     ctx->samples_ready = true;
@@ -455,7 +456,17 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
             ba.gnodes = ctx->gbvh.nodes.as<BvhNode>();
             ba.recs = ctx->grec.as<GaussRec>();
             const int tk = timer_begin(ctx, st, 1);
-            GVC_CUDA(launch_backward_cta(ba, (S + 127) / 128, ctx->blk_desc.as<uint2>(), ctx->blk_boxes.as<float4>(),
+            const int64_t n_blocks = (S + 127) / 128;
+            if (!ctx->blk_b_ready) {
+                GVC_CUDA(ctx->blk_desc_b.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc_b");
+                GVC_CUDA(ctx->blk_boxes_b.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes_b");
+                GVC_CUDA(launch_sample_blocks(S, ctx->s_sorted.as<float4>(), ctx->s_sort.keys.as<uint32_t>(),
+                                              ctx->blk_desc_b.as<uint2>(), ctx->blk_boxes_b.as<float4>(),
+                                              kBlockSplitBackward, st),
+                         "backward block groups");
+                ctx->blk_b_ready = true;
+            }
+            GVC_CUDA(launch_backward_cta(ba, n_blocks, ctx->blk_desc_b.as<uint2>(), ctx->blk_boxes_b.as<float4>(),
                                          st),
                      "backward (tensor core)");
             timer_end(ctx, st, tk);

@@ -97,7 +97,7 @@ __device__ __forceinline__ Box6 rows_box(int a, int b, const float (&x)[4], cons
 // first and last keys differ, taken when both halves' boxes have at most half the
 // half-perimeter of the whole.
 __device__ int rows_split(int a, int b, const uint32_t* keys, const uint32_t (&key)[4], const float (&x)[4],
-                          const float (&y)[4], const float (&z)[4]) {
+                          const float (&y)[4], const float (&z)[4], float ratio) {
     if (b - a < 2) return -1;
     const uint32_t ka = keys[a], kb = keys[b - 1];
     if (ka == kb) return -1;
@@ -115,7 +115,7 @@ __device__ int rows_split(int a, int b, const uint32_t* keys, const uint32_t (&k
     const Box6 B = rows_box(a, b, x, y, z);
     const Box6 B1 = rows_box(a, m, x, y, z);
     const Box6 B2 = rows_box(m, b, x, y, z);
-    return fmaxf(hp6(B1), hp6(B2)) <= 0.5f * hp6(B) ? m : -1;
+    return fmaxf(hp6(B1), hp6(B2)) <= ratio * hp6(B) ? m : -1;
 }
 
 constexpr int kBlocksPerCta = 8;  // 128-row blocks (warps) per CTA of k_sample_blocks
@@ -126,7 +126,7 @@ constexpr int kBlocksPerCta = 8;  // 128-row blocks (warps) per CTA of k_sample_
 __global__ void __launch_bounds__(32 * kBlocksPerCta) k_sample_blocks(const float4* __restrict__ s_sorted,
                                                                       const uint32_t* __restrict__ skeys, int64_t S,
                                                                       int64_t n_blocks, uint2* __restrict__ bdesc,
-                                                                      float4* __restrict__ bboxes) {
+                                                                      float4* __restrict__ bboxes, float ratio) {
     __shared__ uint32_t s_keys[kBlocksPerCta][kBlockRows];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t blk = (int64_t)blockIdx.x * kBlocksPerCta + warp;
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(32 * kBlocksPerCta) k_sample_blocks(const floa
         int na[kBlockGroups], nbb[kBlockGroups];
         int nn = 0;
         for (int i = 0; i < nr; i++) {
-            const int m = rows_split(ra[i], rb[i], keys, key, x, y, z);
+            const int m = rows_split(ra[i], rb[i], keys, key, x, y, z, ratio);
             if (m >= 0) {
                 na[nn] = ra[i];
                 nbb[nn++] = m;
@@ -720,11 +720,11 @@ __global__ void __launch_bounds__((4 / RPT) * 32 + 32,
 static inline unsigned nblk128(int64_t n) { return (unsigned)((n + kBlockRows - 1) / kBlockRows); }
 
 cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32_t* skeys, uint2* bdesc,
-                                 float4* bboxes, cudaStream_t st) {
+                                 float4* bboxes, float ratio, cudaStream_t st) {
     if (S <= 0) return cudaSuccess;
     const int64_t nb = (S + kBlockRows - 1) / kBlockRows;
     k_sample_blocks<<<(unsigned)((nb + kBlocksPerCta - 1) / kBlocksPerCta), 32 * kBlocksPerCta, 0, st>>>(
-        s_sorted, skeys, S, nb, bdesc, bboxes);
+        s_sorted, skeys, S, nb, bdesc, bboxes, ratio);
     gvc::note_launch();
     return cudaGetLastError();
 }

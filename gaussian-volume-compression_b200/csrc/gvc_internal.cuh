@@ -115,6 +115,9 @@ struct gvc_ctx {
                             // (32 if unused), byte 3 = number of groups
     gvc::DevBuf blk_desc;   // [ceil(S/128)] uint2 block-group descriptors (CTA kernels)
     gvc::DevBuf blk_boxes;  // [ceil(S/128) * 8] block-group boxes, 2 x float4
+    gvc::DevBuf blk_desc_b;   // the same with the backward's finer split (built on first use)
+    gvc::DevBuf blk_boxes_b;
+    bool blk_b_ready = false;
     gvc::DevBuf s_grad;     // [n_tiles*32] float4 (x, y, z, gx) backward sample records
     gvc::DevBuf s_gyz;      // [n_tiles*32] float gyz (see k_sample_grads)
     gvc::DevBuf s_ok;       // [n_tiles*32] uint8 1 iff W > 0.01 (pair statistics only)

@@ -60,8 +60,13 @@ struct CtaArgs {
     unsigned long long* stats;
     bool count;
 };
+// Block groups split where both halves' boxes have at most `ratio` of the whole's
+// half-perimeter: kBlockSplitForward for the forward, kBlockSplitBackward (finer) for the
+// tensor-core backward.
+constexpr float kBlockSplitForward = 0.5f;
+constexpr float kBlockSplitBackward = 0.65f;
 cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32_t* skeys, uint2* bdesc,
-                                 float4* bboxes, cudaStream_t st);
+                                 float4* bboxes, float ratio, cudaStream_t st);
 cudaError_t launch_forward_cta(const CtaArgs& a, bool tc, cudaStream_t st);
 cudaError_t launch_tc_gemm_test(const void* A, const void* B, int N, float* D, int* status, cudaStream_t st);
 cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st);
