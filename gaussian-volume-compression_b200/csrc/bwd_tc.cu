@@ -278,7 +278,6 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 bhi = __ldg(rp + 4);
             }
             const GaussB g = gauss_b(r0.x, r0.y, r0.z, r2.z, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, blo, bhi);
-            bool anyc = false;
             bool okc = true;
             for (int q = q0; q <= q1; q++, j++) {
                 const int b = (int)(j & 1u);
@@ -291,19 +290,21 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 }
                 // branch-free over the 16 rows: independent chains the scheduler can interleave
                 // (a per-row warp vote to skip missing rows measured 15 % slower)
+                // rows of the chunk inside the group (warp-uniform bit mask)
+                const int c0 = max(ra - 16 * q, 0), c1 = min(rb - 16 * q, 16);
+                const uint32_t rmask = c1 > c0 ? (((1u << (c1 - c0)) - 1u) << c0) : 0u;
                 float e[16];
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
                     const int r = 16 * q + k;
                     const float4 p = sm.rows[r];
-                    const bool in = r >= ra && r < rb && g.lx <= p.x && p.x <= g.hx && g.ly <= p.y && p.y <= g.hy &&
+                    const bool in = ((rmask >> k) & 1u) && g.lx <= p.x && p.x <= g.hx && g.ly <= p.y && p.y <= g.hy &&
                                     g.lz <= p.z && p.z <= g.hz;
                     const float dx = p.x - g.mx, dy = p.y - g.my, dz = p.z - g.mz;
                     const float p2 = dx * fmaf(g.q0, dx, fmaf(g.q1, dy, g.q2 * dz)) +
                                      dy * fmaf(g.q3, dy, g.q4 * dz) + dz * (g.q5 * dz);
                     const bool c = in && p2 >= kLog2Floor && p2 <= 0.0f;
                     e[k] = c ? ex2_approx(p2) : 0.f;
-                    anyc |= c;
                     if (COUNT) {
                         ncand += in ? 1 : 0;
                         ncontrib += (c && p.w != 0.f) ? 1 : 0;
@@ -338,6 +339,10 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 mbar_arrive(&sm.dfree);
                 mbar_arrive(&sm.empty[s]);
             }
+            // a Gaussian without a contributing pair has an all-zero row of D
+            bool anyc = false;
+#pragma unroll
+            for (int k = 0; k < 20; k++) anyc |= v[k] != 0.f;
             if (anyc) {
                 // moments about the group centre -> moments about the mean (d = u - a)
                 const float ax = g.mx - x0, ay = g.my - y0, az = g.mz - z0;
