@@ -258,6 +258,35 @@ int gvc_sync_status(gvc_ctx* ctx, void* stream) {
     return debug_check(ctx, (cudaStream_t)stream);
 }
 
+// Lane groups of the 32-sample tiles (forward per tile, sample-side backward kernels).
+static int ensure_tile_groups(gvc_ctx* ctx, cudaStream_t st) {
+    if (ctx->tile_groups_ready || ctx->n_tiles == 0) return GVC_OK;
+    const int64_t slots_g = ctx->n_tiles * kGroups;
+    GVC_CUDA(ctx->tile_boxes.ensure(sizeof(float4) * 2 * slots_g), "alloc tile_boxes");
+    GVC_CUDA(ctx->tile_keys.ensure(sizeof(uint32_t) * slots_g), "alloc tile_keys");
+    GVC_CUDA(ctx->tile_gdesc.ensure(sizeof(uint32_t) * ctx->n_tiles), "alloc tile_gdesc");
+    // reads the context's own sorted samples (the caller's array may be gone by now)
+    GVC_CUDA(launch_sample_tiles(ctx->S, ctx->n_tiles, nullptr, nullptr, ctx->s_sort.keys.as<uint32_t>(),
+                                 ctx->s_sorted.as<float4>(),
+                                 ctx->tile_boxes.as<float4>(), ctx->tile_keys.as<uint32_t>(),
+                                 ctx->tile_gdesc.as<uint32_t>(), true, st),
+             "sample tile groups");
+    ctx->tile_groups_ready = true;
+    return GVC_OK;
+}
+
+// The LBVH over the tile lane groups (the deterministic Gaussian-owned backward).
+static int ensure_tile_lbvh(gvc_ctx* ctx, cudaStream_t st) {
+    if (ctx->tiles_ready || ctx->n_tiles == 0) return GVC_OK;
+    const int rc = ensure_tile_groups(ctx, st);
+    if (rc != GVC_OK) return rc;
+    GVC_CUDA(lbvh_hierarchy(ctx->tiles, ctx->n_tiles * kGroups, ctx->tile_keys.as<uint32_t>(),
+                            ctx->tile_boxes.as<float4>(), st),
+             "sample-group LBVH");
+    ctx->tiles_ready = true;
+    return GVC_OK;
+}
+
 int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int use_gaussian_bvh, void* stream) {
     (void)use_gaussian_bvh;  // both reference modes use the same sample ordering here
     if (!ctx) return GVC_ERR_ARG;
@@ -271,21 +300,18 @@ int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int 
     ctx->n_tiles = (S + kTile - 1) / kTile;
     ctx->samples_ready = false;
     ctx->blk_b_ready = false;
+    ctx->tiles_ready = false;        // the sample-group LBVH is built by its first user
+    ctx->tile_groups_ready = false;  // so are the lane groups of the 32-sample tiles
     if (S > 0) {
         GVC_CUDA(morton_sort_points(ctx->s_sort, S, samples, st), "sample sort");
         const int64_t slots = ctx->n_tiles * kTile;
         GVC_CUDA(ctx->s_sorted.ensure(sizeof(float4) * slots), "alloc s_sorted");
-        const int64_t slots_g = ctx->n_tiles * kGroups;
-        GVC_CUDA(ctx->tile_boxes.ensure(sizeof(float4) * 2 * slots_g), "alloc tile_boxes");
-        GVC_CUDA(ctx->tile_keys.ensure(sizeof(uint32_t) * slots_g), "alloc tile_keys");
-        GVC_CUDA(ctx->tile_gdesc.ensure(sizeof(uint32_t) * ctx->n_tiles), "alloc tile_gdesc");
+        // sorted samples only; the 32-sample lane groups and their LBVH are built by their
+        // first user (ensure_tile_groups / ensure_tile_lbvh)
         GVC_CUDA(launch_sample_tiles(S, ctx->n_tiles, samples, ctx->s_sort.perm.as<int32_t>(),
-                                     ctx->s_sort.keys.as<uint32_t>(), ctx->s_sorted.as<float4>(),
-                                     ctx->tile_boxes.as<float4>(), ctx->tile_keys.as<uint32_t>(),
-                                     ctx->tile_gdesc.as<uint32_t>(), st),
+                                     ctx->s_sort.keys.as<uint32_t>(), ctx->s_sorted.as<float4>(), nullptr, nullptr,
+                                     nullptr, false, st),
                  "sample tiles");
-        GVC_CUDA(lbvh_hierarchy(ctx->tiles, slots_g, ctx->tile_keys.as<uint32_t>(), ctx->tile_boxes.as<float4>(), st),
-                 "sample-group LBVH");
         const int64_t n_blocks = (S + 127) / 128;
         GVC_CUDA(ctx->blk_desc.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc");
         GVC_CUDA(ctx->blk_boxes.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes");
@@ -337,6 +363,10 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
                                 ctx->grec.as<GaussRec>(), st),
              "gather records");
     tm.mark();
+    if (ctx->eval_path == 2) {
+        const int rc = ensure_tile_groups(ctx, st);
+        if (rc != GVC_OK) return rc;
+    }
     FwdArgs fa;
     fa.s_sorted = ctx->s_sorted.as<float4>();
     fa.tile_boxes = ctx->tile_boxes.as<float4>();
@@ -435,6 +465,11 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
         ba.s_grad = ctx->s_grad.as<float4>();
         ba.s_gyz = ctx->s_gyz.as<float>();
         ba.s_ok = ctx->s_ok.as<uint8_t>();
+        if (!tc_bwd) {
+            // the deterministic reduction walks the sample groups; the atomic one uses their boxes
+            const int rc = atomic_mode ? ensure_tile_groups(ctx, st) : ensure_tile_lbvh(ctx, st);
+            if (rc != GVC_OK) return rc;
+        }
         ba.tile_boxes = ctx->tile_boxes.as<float4>();
         ba.gdesc = ctx->tile_gdesc.as<uint32_t>();
         ba.n_tiles = ctx->n_tiles;

@@ -118,6 +118,8 @@ struct gvc_ctx {
     gvc::DevBuf blk_desc_b;   // the same with the backward's finer split (built on first use)
     gvc::DevBuf blk_boxes_b;
     bool blk_b_ready = false;
+    bool tiles_ready = false;        // sample-group LBVH built for the current samples
+    bool tile_groups_ready = false;  // tile lane groups built for the current samples
     gvc::DevBuf s_grad;     // [n_tiles*32] float4 (x, y, z, gx) backward sample records
     gvc::DevBuf s_gyz;      // [n_tiles*32] float gyz (see k_sample_grads)
     gvc::DevBuf s_ok;       // [n_tiles*32] uint8 1 iff W > 0.01 (pair statistics only)

@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(256) k_sample_tiles(int64_t S, int64_t n_tiles
                                                       const int32_t* __restrict__ perm,
                                                       const uint32_t* __restrict__ skeys, float4* __restrict__ s_sorted,
                                                       float4* __restrict__ group_boxes, uint32_t* __restrict__ group_keys,
-                                                      uint32_t* __restrict__ gdesc) {
+                                                      uint32_t* __restrict__ gdesc, int with_groups) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t t = i >> 5;
     if (t >= n_tiles) return;
@@ -233,14 +233,24 @@ __global__ void __launch_bounds__(256) k_sample_tiles(int64_t S, int64_t n_tiles
     float x = NAN, y = NAN, z = NAN;
     int o = -1;
     uint32_t key = 0xffffffffu;
-    if (i < S) {
-        o = perm[i];
-        x = samples[3 * (int64_t)o];
-        y = samples[3 * (int64_t)o + 1];
-        z = samples[3 * (int64_t)o + 2];
-        key = skeys[i];
+    if (!with_groups) {
+        // pass 1 (build_bvh): gather the sorted samples
+        if (i < S) {
+            o = perm[i];
+            x = samples[3 * (int64_t)o];
+            y = samples[3 * (int64_t)o + 1];
+            z = samples[3 * (int64_t)o + 2];
+        }
+        s_sorted[i] = make_float4(x, y, z, __int_as_float(o));
+        return;  // warp-uniform
     }
-    s_sorted[i] = make_float4(x, y, z, __int_as_float(o));
+    // pass 2 (first user of the lane groups): read them back from s_sorted
+    const float4 sp = s_sorted[i];
+    x = sp.x;
+    y = sp.y;
+    z = sp.z;
+    o = __float_as_int(sp.w);
+    if (i < S) key = skeys[i];
     const int nvalid = __popc(__ballot_sync(0xffffffffu, o >= 0));
     int starts[kGroups + 1];
     int ng = 1;
@@ -330,10 +340,10 @@ cudaError_t launch_gather_recs(int64_t P, const int32_t* perm, const float* mean
 
 cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples, const int32_t* perm,
                                 const uint32_t* skeys, float4* s_sorted, float4* group_boxes, uint32_t* group_keys,
-                                uint32_t* gdesc, cudaStream_t st) {
+                                uint32_t* gdesc, bool with_groups, cudaStream_t st) {
     if (n_tiles <= 0) return cudaSuccess;
     k_sample_tiles<<<nb256(n_tiles * 32), 256, 0, st>>>(S, n_tiles, samples, perm, skeys, s_sorted, group_boxes,
-                                                        group_keys, gdesc); gvc::note_launch();
+                                                        group_keys, gdesc, with_groups ? 1 : 0); gvc::note_launch();
     return cudaGetLastError();
 }
 

@@ -86,7 +86,7 @@ cudaError_t launch_gather_recs(int64_t P, const int32_t* perm, const float* mean
                                cudaStream_t st);
 cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples, const int32_t* perm,
                                 const uint32_t* skeys, float4* s_sorted, float4* group_boxes, uint32_t* group_keys,
-                                uint32_t* gdesc, cudaStream_t st);
+                                uint32_t* gdesc, bool with_groups, cudaStream_t st);
 cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float* out_cells,
                                 const float* out_weights, const float* gout, const float* gw, float4* s_grad,
                                 float* s_gyz, uint8_t* s_ok, cudaStream_t st);
