@@ -2,7 +2,7 @@
 """Benchmark of the Gaussian-mixture volume training step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config large|medium|small|slice|tiny] [--eval-path plain|tensor_core|plain_tile] [--mesh]
+                    [--config large|medium|small|slice|tiny] [--eval-path plain|tensor_core|plain_tile] [--mesh] [--knn]
 
 Default configuration: FP32 forward (CTA pipeline) and the tensor-core backward reduction
 (--bwd-mode tensor_core); tc_vs_plain times FP32 throughout (the library default) and
@@ -77,6 +77,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile", action="store_true", help="minimal run for ncu (no e2e, no CPU baseline)")
+    p.add_argument("--knn", action="store_true",
+                   help="also time distCUDA2 (3-NN mean squared distance) on the 2M clustered Gaussian means "
+                        "and add a knn3 object")
     p.add_argument("--mesh", action="store_true",
                    help="also time the mesh samplers (128^3 jittered hex grid split into 12.6M tetrahedra, "
                         "256^3 uniform grid, 8M points each) and add a mesh_sampler object")
@@ -326,6 +329,41 @@ def mesh_bench(dev, steps, warmup, with_cpu):
 
 
 # ----------------------------------------------------------------------------------------
+# Three-nearest-neighbour distances (distCUDA2 drop-in): device-resident points
+# ----------------------------------------------------------------------------------------
+def knn_bench(dev, means, steps, warmup, with_cpu):
+    import torch
+    from simple_knn._C import distCUDA2
+    pts = means.to(dev).contiguous()
+    n = int(pts.shape[0])
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        distCUDA2(pts)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        out = distCUDA2(pts)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    res = {"points": n, "ms_per_call": ms, "points_per_s": n / (ms * 1e-3),
+           "includes": "point LBVH build (keys, sort, Karras, refit) + exact 3-NN traversal",
+           "points_desc": "Gaussian means of the headline workload (256 clusters)"}
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        host = pts.cpu().numpy()
+        t0 = time.perf_counter()
+        ref = oracle.knn3_mean_dist2(host)
+        t = time.perf_counter() - t0
+        res["bit_exact_vs_oracle"] = bool(np.array_equal(ref, out.cpu().numpy()))
+        res["cpu_oracle"] = {"ms_per_call": t * 1e3, "cores": os.cpu_count() or 1,
+                             "sample": "oracle (C, OpenMP, uniform grid) on all %d points" % n}
+    return res
+
+
+# ----------------------------------------------------------------------------------------
 # Our arm
 # ----------------------------------------------------------------------------------------
 def run_ours(args):
@@ -555,6 +593,8 @@ def run_ours(args):
                            else "single GPU"},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e, "tc_vs_plain": tc_vs_plain,
                 "gpu_launches": int(launches), "gpu_launches_per_step": launches / args.steps}
+        if args.knn and world == 1:
+            line["knn3"] = knn_bench(dev, d_means, 10, 3, not args.no_cpu_baseline)
         if args.mesh and world == 1:
             line["mesh_sampler"] = mesh_bench(dev, 5, 2, not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)

@@ -28,6 +28,7 @@ SOURCES = {
     "noalloc.cu": [],
     "cta.cu": [],
     "bwd_tc.cu": [],
+    "knn.cu": [],
 }
 
 

@@ -179,14 +179,14 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(c->device);
-    Lbvh* lbvhs[] = {&c->s_sort, &c->tiles, &c->gbvh, &c->cells, &c->scratch.dbg, &c->scratch.msamp};
+    Lbvh* lbvhs[] = {&c->s_sort, &c->tiles, &c->gbvh, &c->cells, &c->knn, &c->scratch.dbg, &c->scratch.msamp};
     for (Lbvh* L : lbvhs) {
         DevBuf* bufs[] = {&L->keys, &L->keys_alt, &L->perm, &L->perm_alt, &L->boxes, &L->sorted_boxes, &L->left,
                           &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds};
         for (DevBuf* b : bufs) b->release();
     }
     DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->blk_desc_b, &c->blk_boxes_b, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
-                      &c->m_out_sorted, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
+                      &c->m_out_sorted, &c->knn_boxes, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
     for (DevBuf* b : bufs) b->release();
     if (c->d_status) cudaFree(c->d_status);
     if (c->d_stats) cudaFree(c->d_stats);
@@ -581,6 +581,22 @@ int gvc_sample_tets(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, con
     GVC_CUDA(launch_sample_tets(N, samples, sc->msamp.perm.as<int32_t>(), pts, conn4, values, cnodes, cperm, C, out,
                                 cell_ids, ctx->d_status, st),
              "sample tets");
+    return GVC_OK;
+}
+
+int gvc_knn3_mean_dist2(gvc_ctx* ctx, int64_t n, const float* pts, float* out, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (n < 0) return fail(ctx, GVC_ERR_ARG, "negative point count");
+    if (n > kMaxElems) return fail(ctx, GVC_ERR_CAPACITY, "point count out of range");
+    if (n == 0) return GVC_OK;
+    if (!pts || !out) return fail(ctx, GVC_ERR_ARG, "null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    GVC_CUDA(ctx->knn_boxes.ensure(sizeof(float4) * 2 * n), "alloc point boxes");
+    GVC_CUDA(launch_point_boxes(n, pts, ctx->knn_boxes.as<float4>(), st), "point boxes");
+    GVC_CUDA(lbvh_build_boxes(ctx->knn, n, ctx->knn_boxes.as<float4>(), st), "point LBVH");
+    GVC_CUDA(launch_knn3(n, ctx->knn.sorted_boxes.as<float4>(), ctx->knn.perm.as<int32_t>(),
+                         ctx->knn.nodes.as<BvhNode>(), out, ctx->d_status, st),
+             "knn3");
     return GVC_OK;
 }
 

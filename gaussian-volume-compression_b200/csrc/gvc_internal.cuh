@@ -133,6 +133,9 @@ struct gvc_ctx {
     gvc::DevBuf gtmp;       // preprocess scratch: AABBs in caller order
     // mesh sampler
     gvc::Lbvh cells;
+    // three-nearest-neighbour distances (point LBVH and its leaf boxes)
+    gvc::Lbvh knn;
+    gvc::DevBuf knn_boxes;
     gvc::DevBuf m_out_sorted;
     // status and statistics
     int* d_status = nullptr;          // device status word

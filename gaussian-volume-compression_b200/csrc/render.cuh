@@ -108,4 +108,9 @@ cudaError_t launch_sample_tets(int64_t N, const float* samples, const int32_t* s
                                const int32_t* cperm, int64_t C, double* out, int64_t* cell_ids, int* status,
                                cudaStream_t st);
 
+// knn.cu
+cudaError_t launch_point_boxes(int64_t n, const float* pts, float4* boxes, cudaStream_t st);
+cudaError_t launch_knn3(int64_t n, const float4* sorted_boxes, const int32_t* perm, const BvhNode* nodes, float* out,
+                        int* status, cudaStream_t st);
+
 }  // namespace gvc

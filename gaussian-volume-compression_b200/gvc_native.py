@@ -42,6 +42,7 @@ _SIGNATURES = {
     "gvc_sample_uniform": [_vp, _vp, _vp, _vp, _vp, _int, _i64, _vp, _vp, _vp],
     "gvc_sample_tets": [_vp, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp, _vp],
     "gvc_sample_cells": [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp],
+    "gvc_knn3_mean_dist2": [_vp, _i64, _vp, _vp, _vp],
     "gvc_debug_lbvh": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "gvc_debug_preprocess": [_vp, _i64, _vp, _vp, _vp, _vp, _f32, _vp, _vp, _vp],
     "gvc_debug_sample_order": [_vp, _vp, _vp, _vp],

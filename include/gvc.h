@@ -152,6 +152,17 @@ int gvc_sample_cells(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, co
                      const int64_t* cell_offsets, const int32_t* conn, const double* values, int64_t N,
                      const float* samples, double* out, int64_t* cell_ids, void* stream);
 
+/* Mean squared distance to the three nearest other points, one value per point: the
+   initial Gaussian scale rule, replacing simple-knn's distCUDA2 (a third-party
+   extension outside the reference tree, called at scene/gaussian_model.py:175-179 and
+   :729-733).  pts [n][3] float32, out [n] float32, both device pointers.  Exact: the
+   three smallest float32 squared distances ((dx*dx + dy*dy) + dz*dz, each operation
+   rounded) to any other index, summed in ascending order and divided by 3 in float32;
+   when fewer than three other points exist the missing ones count as FLT_MAX (so n <= 2
+   gives +inf).  A traversal overflow (impossible for the LBVH's depth) is reported by
+   gvc_sync_status. */
+int gvc_knn3_mean_dist2(gvc_ctx* ctx, int64_t n, const float* pts, float* out, void* stream);
+
 /* No counterpart in the reference.  Tetrahedral sampling for callers that cannot
    allocate device memory (their memory belongs to another allocator, or cudaMalloc's
    device-wide synchronisation is unacceptable where they call).  Same inputs, outputs

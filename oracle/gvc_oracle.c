@@ -18,6 +18,7 @@
  * reference project).  Compile with -ffp-contract=off so that the double-precision
  * predicates match the GPU's explicitly rounded arithmetic bit for bit.
  */
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -1170,4 +1171,126 @@ void orc_sample_cells(int64_t npts, const float* pts, int64_t C, const uint8_t* 
     }
     grid_free(&g);
     free(boxes);
+}
+
+/* ------------------------------------------------------------------------------------
+ * Three-nearest-neighbour mean squared distance: the initial Gaussian scale rule of
+ * scene/gaussian_model.py:175-179 (create_from_pcd) and :729-733 (densify_in_empty),
+ * which call simple-knn's distCUDA2 (third-party, not in the reference tree).  Its
+ * published behaviour: per point, the three smallest squared distances to any OTHER
+ * index (duplicates count with distance 0), ascending, summed (b0 + b1) + b2 and
+ * divided by 3 in float32; missing neighbours count as FLT_MAX.  The squared distance
+ * is (dx*dx + dy*dy) + dz*dz in float32 with every operation rounded (no contraction).
+ *
+ * Search: exact, on a uniform grid of about n/2 cells (at most 1001 per axis); rings of
+ * cells around the query's cell are scanned until the distance from the query to the
+ * outside of the scanned block (in double, less a relative margin far above float
+ * rounding) exceeds the current third-best distance.
+ * ------------------------------------------------------------------------------------ */
+static inline float knn_d2(const float* a, const float* b) {
+    float dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    float xx = dx * dx, yy = dy * dy, zz = dz * dz;
+    float s = xx + yy;
+    return s + zz;
+}
+
+static inline void knn_keep3(float d, float* b) {
+    if (d < b[2]) {
+        if (d < b[1]) {
+            b[2] = b[1];
+            if (d < b[0]) { b[1] = b[0]; b[0] = d; } else { b[1] = d; }
+        } else {
+            b[2] = d;
+        }
+    }
+}
+
+void orc_knn3_mean_dist2(int64_t n, const float* pts, float* out, int nthreads) {
+    int nt = orc_nthreads(nthreads);
+    if (n <= 0) return;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = 0; i < n; i++)
+        for (int a = 0; a < 3; a++) {
+            double v = pts[3 * i + a];
+            if (v < lo[a]) lo[a] = v;
+            if (v > hi[a]) hi[a] = v;
+        }
+    double ext = 0.0;
+    for (int a = 0; a < 3; a++) ext = fmax(ext, hi[a] - lo[a]);
+    if (!(ext > 0.0)) ext = 1.0;
+    /* cubic cells of side h, about n/2 cells over the bounding box */
+    double vol = 1.0;
+    for (int a = 0; a < 3; a++) vol *= fmax(hi[a] - lo[a], ext * 1e-3);
+    double h = cbrt(vol / fmax(1.0, 0.5 * (double)n));
+    if (!(h > 0.0)) h = ext;
+    for (int a = 0; a < 3; a++) h = fmax(h, (hi[a] - lo[a]) / 1000.0);
+    int64_t dim[3];
+    for (int a = 0; a < 3; a++) dim[a] = (int64_t)(floor((hi[a] - lo[a]) / h) + 1.0);
+    int64_t ncell = dim[0] * dim[1] * dim[2];
+    int64_t* start = (int64_t*)calloc((size_t)ncell + 1, sizeof(int64_t));
+    int64_t* cellof = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+    int64_t* items = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+        int64_t c[3];
+        for (int a = 0; a < 3; a++) {
+            double f = floor(((double)pts[3 * i + a] - lo[a]) / h);
+            c[a] = clampi((int64_t)f, 0, dim[a] - 1);
+        }
+        cellof[i] = (c[2] * dim[1] + c[1]) * dim[0] + c[0];
+        start[cellof[i] + 1]++;
+    }
+    for (int64_t c = 0; c < ncell; c++) start[c + 1] += start[c];
+    {
+        int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)ncell);
+        memcpy(fill, start, sizeof(int64_t) * (size_t)ncell);
+        for (int64_t i = 0; i < n; i++) items[fill[cellof[i]]++] = i;
+        free(fill);
+    }
+    int64_t rmax = dim[0];
+    if (dim[1] > rmax) rmax = dim[1];
+    if (dim[2] > rmax) rmax = dim[2];
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; i++) {
+        const float* q = pts + 3 * i;
+        int64_t c[3];
+        c[0] = cellof[i] % dim[0];
+        c[1] = (cellof[i] / dim[0]) % dim[1];
+        c[2] = cellof[i] / (dim[0] * dim[1]);
+        float b[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+        for (int64_t r = 0; r <= rmax; r++) {
+            for (int64_t z = c[2] - r; z <= c[2] + r; z++) {
+                if (z < 0 || z >= dim[2]) continue;
+                for (int64_t y = c[1] - r; y <= c[1] + r; y++) {
+                    if (y < 0 || y >= dim[1]) continue;
+                    int shell_zy = (z == c[2] - r || z == c[2] + r || y == c[1] - r || y == c[1] + r);
+                    for (int64_t x = c[0] - r; x <= c[0] + r; x++) {
+                        if (x < 0 || x >= dim[0]) continue;
+                        if (!shell_zy && x != c[0] - r && x != c[0] + r) continue;
+                        int64_t cl = (z * dim[1] + y) * dim[0] + x;
+                        for (int64_t k = start[cl]; k < start[cl + 1]; k++) {
+                            int64_t j = items[k];
+                            if (j == i) continue;
+                            knn_keep3(knn_d2(q, pts + 3 * j), b);
+                        }
+                    }
+                }
+            }
+            /* distance from q to the outside of the scanned block of cells */
+            double m = INFINITY;
+            int covers = 1;
+            for (int a = 0; a < 3; a++) {
+                int64_t c0 = c[a] - r, c1 = c[a] + r;
+                if (c0 > 0) { m = fmin(m, (double)q[a] - (lo[a] + (double)c0 * h)); covers = 0; }
+                if (c1 < dim[a] - 1) { m = fmin(m, lo[a] + (double)(c1 + 1) * h - (double)q[a]); covers = 0; }
+            }
+            if (covers) break;
+            if (m > 0.0 && (double)b[2] < m * m * (1.0 - 1e-5)) break;
+        }
+        float s = b[0] + b[1];
+        s = s + b[2];
+        out[i] = s / 3.0f;
+    }
+    free(start);
+    free(cellof);
+    free(items);
 }

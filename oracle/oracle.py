@@ -59,6 +59,7 @@ def lib():
             "orc_sample_tets": [i64, vp, i64, vp, vp, i64, vp, vp, vp, i32],
             "orc_tet_boxes": [i64, vp, vp, vp],
             "orc_sample_cells": [i64, vp, i64, vp, vp, vp, vp, i64, vp, vp, vp, i32],
+            "orc_knn3_mean_dist2": [i64, vp, vp, i32],
             "orc_openmp_enabled": [],
         }
         for name, args in sig.items():
@@ -235,6 +236,15 @@ def sample_cells(pts, types, offsets, conn, values, samples, nthreads=0):
     lib().orc_sample_cells(pts.shape[0], _p(pts), types.shape[0], _p(types), _p(offsets), _p(conn), _p(values), n,
                            _p(samples), _p(out), _p(cell), nthreads)
     return out, cell
+
+
+def knn3_mean_dist2(pts, nthreads=0):
+    """Mean squared distance to the three nearest other points, float32 (the initial
+    scale rule of scene/gaussian_model.py:175-179, :729-733; simple-knn distCUDA2)."""
+    pts = _c(pts, np.float32).reshape(-1, 3)
+    out = np.zeros(pts.shape[0], np.float32)
+    lib().orc_knn3_mean_dist2(pts.shape[0], _p(pts), _p(out), nthreads)
+    return out
 
 
 # --------------------------------------------------------------------------------------
