@@ -312,6 +312,28 @@ def mesh_bench(dev, steps, warmup, with_cpu):
                              "sample": "oracle (C, OpenMP, uniform grid locator) on 1M of the points, "
                                        "locator build included (%.2f s)" % t}
     res["tets"] = tet
+    # training batches (train.py:34-61, :273-315): 100 batches of 128^3 points in random
+    # tetrahedra, per-batch Morton sort, float32 ground truth, all on the device
+    B, S = 100, 128 ** 3
+    d_bs = torch.empty((B, S, 3), dtype=torch.float32, device=dev)
+    d_bg = torch.empty((B, S), dtype=torch.float32, device=dev)
+    ms = timed(lambda: ctx.call("gvc_training_samples", pts.shape[0], gvc_native.ptr(d_pts), tets.shape[0],
+                                gvc_native.ptr(d_tets), gvc_native.ptr(d_vals), B, S, ctypes.c_uint64(0),
+                                gvc_native.ptr(d_bs), gvc_native.ptr(d_bg), sp))
+    tb = {"batches": B, "batch_size": S, "cells": int(tets.shape[0]), "ms_per_call": ms,
+          "points_per_s": B * S / (ms * 1e-3),
+          "includes": "Philox points in random tets + 3-word radix sort (batch, 63-bit Morton) + gather "
+                      "+ cell LBVH build + locate + interpolate + float32 conversion",
+          "found": float((d_bg[:4] != -1).float().mean().item())}
+    del d_bs, d_bg
+    if with_cpu:
+        t0 = time.perf_counter()
+        oracle.training_samples(pts, tets, vals, 1, 2_000_000, seed=0)
+        t = time.perf_counter() - t0
+        tb["cpu_oracle"] = {"points_per_s": 2_000_000 / t, "cores": os.cpu_count() or 1,
+                            "sample": "oracle (C Philox points, numpy stable Morton sort, C grid locator) on "
+                                      "one batch of 2M points (%.2f s)" % t}
+    res["training_batches"] = tb
     del d_pts, d_tets, d_vals
     # uniform grid: 256^3 float32 point values, trilinear, 8M points
     dims = np.array([256, 256, 256], np.int64)

@@ -29,6 +29,7 @@ SOURCES = {
     "cta.cu": [],
     "bwd_tc.cu": [],
     "knn.cu": [],
+    "trainsamp.cu": [],
 }
 
 

@@ -179,14 +179,15 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(c->device);
-    Lbvh* lbvhs[] = {&c->s_sort, &c->tiles, &c->gbvh, &c->cells, &c->knn, &c->scratch.dbg, &c->scratch.msamp};
+    Lbvh* lbvhs[] = {&c->s_sort,  &c->tiles,      &c->gbvh,          &c->cells,
+                     &c->knn,     &c->ts_sort,    &c->scratch.dbg,   &c->scratch.msamp};
     for (Lbvh* L : lbvhs) {
         DevBuf* bufs[] = {&L->keys, &L->keys_alt, &L->perm, &L->perm_alt, &L->boxes, &L->sorted_boxes, &L->left,
                           &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds};
         for (DevBuf* b : bufs) b->release();
     }
     DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->blk_desc_b, &c->blk_boxes_b, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
-                      &c->m_out_sorted, &c->knn_boxes, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
+                      &c->m_out_sorted, &c->knn_boxes, &c->ts_points, &c->ts_words, &c->ts_gt64, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
     for (DevBuf* b : bufs) b->release();
     if (c->d_status) cudaFree(c->d_status);
     if (c->d_stats) cudaFree(c->d_stats);
@@ -597,6 +598,47 @@ int gvc_knn3_mean_dist2(gvc_ctx* ctx, int64_t n, const float* pts, float* out, v
     GVC_CUDA(launch_knn3(n, ctx->knn.sorted_boxes.as<float4>(), ctx->knn.perm.as<int32_t>(),
                          ctx->knn.nodes.as<BvhNode>(), out, ctx->d_status, st),
              "knn3");
+    return GVC_OK;
+}
+
+int gvc_training_samples(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, const int32_t* conn4,
+                         const double* values, int64_t num_batches, int64_t batch_size, uint64_t seed,
+                         float* samples_out, float* gt_out, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    if (npts < 0 || C < 0 || num_batches < 0 || batch_size < 0) return fail(ctx, GVC_ERR_ARG, "negative size");
+    if (C == 0 || npts == 0) return fail(ctx, GVC_ERR_ARG, "the mesh has no cells or no points");
+    if (num_batches == 0 || batch_size == 0) return GVC_OK;
+    if (C > kMaxElems || batch_size > kMaxElems || num_batches > kMaxElems / batch_size)
+        return fail(ctx, GVC_ERR_CAPACITY, "num_batches * batch_size out of range");
+    if (!pts || !conn4 || !samples_out || (gt_out && !values)) return fail(ctx, GVC_ERR_ARG, "null pointer");
+    const int64_t N = num_batches * batch_size;
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch* sc = scratch_of(ctx);
+    GVC_CUDA(ctx->ts_points.ensure(sizeof(float) * 3 * N), "alloc sample points");
+    GVC_CUDA(ctx->ts_words.ensure(sizeof(uint32_t) * 3 * N), "alloc sort keys");
+    uint32_t* w = ctx->ts_words.as<uint32_t>();
+    GVC_CUDA(launch_tet_points(N, batch_size, seed, pts, conn4, C, ctx->ts_points.as<float>(), w, w + N, w + 2 * N,
+                               st),
+             "tet points");
+    // batch index most significant, then the 63-bit Morton code (high word, low word)
+    int batch_bits = 0;
+    while (batch_bits < 32 && (uint64_t(1) << batch_bits) < (uint64_t)num_batches) batch_bits++;
+    const uint32_t* words[3] = {w, w + N, w + 2 * N};
+    const int bits[3] = {32, 31, batch_bits};
+    GVC_CUDA(radix_sort_words(ctx->ts_sort, N, words, bits, batch_bits > 0 ? 3 : 2, st), "batch Morton sort");
+    GVC_CUDA(launch_gather_points(N, ctx->ts_points.as<float>(), ctx->ts_sort.perm.as<int32_t>(), samples_out, st),
+             "gather samples");
+    if (!gt_out) return GVC_OK;
+    GVC_CUDA(sc->tmp_boxes.ensure(sizeof(float4) * 2 * C), "alloc cell boxes");
+    GVC_CUDA(launch_tet_boxes(C, pts, conn4, sc->tmp_boxes.as<float4>(), st), "tet boxes");
+    GVC_CUDA(lbvh_build_boxes(ctx->cells, C, sc->tmp_boxes.as<float4>(), st), "cell LBVH");
+    GVC_CUDA(ctx->ts_gt64.ensure(sizeof(double) * N), "alloc values");
+    // the samples are Morton-sorted per batch already: locate them in that order
+    GVC_CUDA(launch_sample_tets(N, samples_out, nullptr, pts, conn4, values, ctx->cells.nodes.as<BvhNode>(),
+                                ctx->cells.perm.as<int32_t>(), C, ctx->ts_gt64.as<double>(), nullptr,
+                                ctx->d_status, st),
+             "sample tets");
+    GVC_CUDA(launch_to_f32(N, ctx->ts_gt64.as<double>(), gt_out, st), "values to float32");
     return GVC_OK;
 }
 

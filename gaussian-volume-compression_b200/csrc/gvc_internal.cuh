@@ -136,6 +136,9 @@ struct gvc_ctx {
     // three-nearest-neighbour distances (point LBVH and its leaf boxes)
     gvc::Lbvh knn;
     gvc::DevBuf knn_boxes;
+    // training sample batches: unsorted points, Morton / batch key words, FP64 values
+    gvc::Lbvh ts_sort;
+    gvc::DevBuf ts_points, ts_words, ts_gt64;
     gvc::DevBuf m_out_sorted;
     // status and statistics
     int* d_status = nullptr;          // device status word

@@ -333,6 +333,58 @@ cudaError_t radix_sort_pairs(Lbvh& L, int64_t n, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+__global__ void __launch_bounds__(256) k_gather_u32(int64_t n, const uint32_t* __restrict__ src,
+                                                    const int32_t* __restrict__ perm, uint32_t* __restrict__ dst) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[perm[i]];
+}
+
+cudaError_t radix_sort_words(Lbvh& L, int64_t n, const uint32_t* const* words, const int* bits, int nwords,
+                             cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int nb = (int)((n + kRsTile - 1) / kRsTile);
+    cudaError_t e;
+    if ((e = L.keys.ensure(sizeof(uint32_t) * n)) != cudaSuccess) return e;
+    if ((e = L.keys_alt.ensure(sizeof(uint32_t) * n)) != cudaSuccess) return e;
+    if ((e = L.perm.ensure(sizeof(int32_t) * n)) != cudaSuccess) return e;
+    if ((e = L.perm_alt.ensure(sizeof(int32_t) * n)) != cudaSuccess) return e;
+    if ((e = L.hist.ensure(sizeof(uint32_t) * (256 * (size_t)nb + 256))) != cudaSuccess) return e;
+    uint32_t* hist = L.hist.as<uint32_t>();
+    uint32_t* totals = hist + 256 * (size_t)nb;
+    uint32_t* kin = L.keys.as<uint32_t>();
+    uint32_t* kout = L.keys_alt.as<uint32_t>();
+    int32_t* vin = nullptr;  // identity before the first pass
+    int32_t* vout = L.perm_alt.as<int32_t>();
+    const unsigned gb = (unsigned)((n + 255) / 256);
+    for (int w = 0; w < nwords; w++) {
+        const int passes = (bits[w] + 7) / 8;
+        if (passes <= 0) continue;
+        // this word's keys in the current order
+        if (vin) {
+            k_gather_u32<<<gb, 256, 0, st>>>(n, words[w], vin, kin); gvc::note_launch();
+        } else if ((e = cudaMemcpyAsync(kin, words[w], sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st)) !=
+                   cudaSuccess) {
+            return e;
+        }
+        for (int pass = 0; pass < passes; pass++) {
+            k_rs_hist<<<nb, 256, 0, st>>>(kin, n, nb, pass, hist); gvc::note_launch();
+            k_rs_scan<<<256, 1024, 0, st>>>(hist, nb, totals); gvc::note_launch();
+            k_rs_scatter<<<nb, 256, 0, st>>>(kin, vin, kout, vout, n, nb, pass, hist, totals); gvc::note_launch();
+            uint32_t* tk = kin;
+            kin = kout;
+            kout = tk;
+            int32_t* tv = vin;
+            vin = vout;
+            vout = tv ? tv : (vin == L.perm_alt.as<int32_t>() ? L.perm.as<int32_t>() : L.perm_alt.as<int32_t>());
+        }
+    }
+    if (!vin) return cudaErrorInvalidValue;  // no word had any bits
+    if (vin != L.perm.as<int32_t>() &&
+        (e = cudaMemcpyAsync(L.perm.ptr, vin, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+        return e;
+    return cudaGetLastError();
+}
+
 // ----------------------------------------------------------------------------------
 // Karras 2012 ("Maximizing parallelism in the construction of BVHs, octrees and k-d
 // trees", HPG 2012, Fig. 4).  Equal keys are disambiguated by position.

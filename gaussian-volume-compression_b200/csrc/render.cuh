@@ -108,6 +108,12 @@ cudaError_t launch_sample_tets(int64_t N, const float* samples, const int32_t* s
                                const int32_t* cperm, int64_t C, double* out, int64_t* cell_ids, int* status,
                                cudaStream_t st);
 
+// trainsamp.cu
+cudaError_t launch_tet_points(int64_t N, int64_t S, uint64_t seed, const float* pts, const int32_t* conn4, int64_t C,
+                              float* out, uint32_t* w_lo, uint32_t* w_hi, uint32_t* w_batch, cudaStream_t st);
+cudaError_t launch_gather_points(int64_t N, const float* src, const int32_t* perm, float* dst, cudaStream_t st);
+cudaError_t launch_to_f32(int64_t N, const double* src, float* dst, cudaStream_t st);
+
 // knn.cu
 cudaError_t launch_point_boxes(int64_t n, const float* pts, float4* boxes, cudaStream_t st);
 cudaError_t launch_knn3(int64_t n, const float4* sorted_boxes, const int32_t* perm, const BvhNode* nodes, float* out,

@@ -1,7 +1,7 @@
 """Drop-in replacement of the reference package gpu_mesh_sampling
 (gpu_sampling/gpu_mesh_sampling/__init__.py): numpy in, numpy out, sampling on the GPU
 through libgvc.so."""
-from ._gpu_mesh_sampling import sample_mesh, sample_meshu
+from ._gpu_mesh_sampling import sample_mesh, sample_meshu, sample_training_batches  # noqa: F401
 import numpy as np
 
 

@@ -186,3 +186,56 @@ def sample_meshu(pts_arr, conn_arr, cell_types_arr, cell_offsets_arr, val_arr, s
         return out
     out, _ = sample_meshu_mixed(pts_arr, conn_arr, cell_types_arr, cell_offsets_arr, val_arr, samp_arr)
     return out
+
+
+def sample_training_batches(pts_arr, tets_arr, val_arr, num_batches, batch_size, seed=0, gt_cells=None):
+    """Training batches built on the device (train.py:34-61 sample_mesh_points, :273-282
+    ground truth through gpu_sampleu, :286-315 per-batch Morton sort).
+
+    pts [Np,3] and val [Np] are the mesh's points and point field; tets [C,4] the vertex
+    ids of its tetrahedra (the reference's `mesh.triangulate()`).  Points are drawn
+    uniformly over cells and inside each by sorted-uniform barycentric weights (Philox
+    keyed by `seed`), sorted per batch by their clamped 21-bit Morton code, and sampled for
+    the ground truth.  gt_cells = (conn, cell_types, cell_offsets) takes the ground truth
+    from that (untriangulated) cell mesh instead, as the reference does when it samples
+    the original mesh.  Returns CUDA tensors (samples [B,S,3] float32, gt [B,S] float32);
+    nothing goes through host memory after the mesh upload.
+    """
+    pts = np.ascontiguousarray(pts_arr, dtype=np.float32).reshape(-1, 3)
+    tets = np.ascontiguousarray(tets_arr, dtype=np.int64).reshape(-1, 4)
+    vals = np.ascontiguousarray(val_arr, dtype=np.float64).reshape(-1)
+    B, S = int(num_batches), int(batch_size)
+    if B < 0 or S < 0:
+        raise RuntimeError("num_batches and batch_size must be non-negative")
+    if tets.shape[0] == 0 or pts.shape[0] == 0:
+        raise RuntimeError("the mesh has no cells or no points")
+    if tets.min() < 0 or tets.max() >= pts.shape[0]:
+        raise RuntimeError("connectivity refers to a point outside the point array")
+    if vals.size < pts.shape[0]:
+        raise RuntimeError("values must hold one entry per point")
+    dev, c = _ctx()
+    d = "cuda:%d" % dev
+    samples = torch.empty((B, S, 3), dtype=torch.float32, device=d)
+    gt = torch.empty((B, S), dtype=torch.float32, device=d)
+    if B * S == 0:
+        return samples, gt
+    d_pts = _dev(pts, np.float32)
+    d_tets = _dev(tets, np.int32)
+    d_vals = _dev(vals, np.float64)
+    c.call("gvc_training_samples", pts.shape[0], _n.ptr(d_pts), tets.shape[0], _n.ptr(d_tets), _n.ptr(d_vals),
+           B, S, ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), _n.ptr(samples),
+           None if gt_cells is not None else _n.ptr(gt), _stream(dev))
+    if gt_cells is not None:
+        conn, types, offs = _check_cells(*gt_cells)
+        if conn.size and (conn.min() < 0 or conn.max() >= pts.shape[0]):
+            raise RuntimeError("connectivity refers to a point outside the point array")
+        C = types.size
+        d_conn = _dev(conn if conn.size else np.zeros(1, np.int32), np.int32)
+        d_types = _dev(types if C else np.zeros(1, np.uint8), np.uint8)
+        d_offs = _dev(offs if C else np.zeros(1, np.int64), np.int64)
+        g64 = torch.empty(B * S, dtype=torch.float64, device=d)
+        c.call("gvc_sample_cells", pts.shape[0], _n.ptr(d_pts), C, _n.ptr(d_types), _n.ptr(d_offs), _n.ptr(d_conn),
+               _n.ptr(d_vals), B * S, _n.ptr(samples), _n.ptr(g64), None, _stream(dev))
+        gt.copy_(g64.view(B, S))
+    c.sync_status(torch.cuda.current_stream(dev).cuda_stream)
+    return samples, gt

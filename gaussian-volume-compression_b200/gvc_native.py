@@ -43,6 +43,7 @@ _SIGNATURES = {
     "gvc_sample_tets": [_vp, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp, _vp],
     "gvc_sample_cells": [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp],
     "gvc_knn3_mean_dist2": [_vp, _i64, _vp, _vp, _vp],
+    "gvc_training_samples": [_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, ctypes.c_uint64, _vp, _vp, _vp],
     "gvc_debug_lbvh": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "gvc_debug_preprocess": [_vp, _i64, _vp, _vp, _vp, _vp, _f32, _vp, _vp, _vp],
     "gvc_debug_sample_order": [_vp, _vp, _vp, _vp],

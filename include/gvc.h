@@ -163,6 +163,20 @@ int gvc_sample_cells(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, co
    gvc_sync_status. */
 int gvc_knn3_mean_dist2(gvc_ctx* ctx, int64_t n, const float* pts, float* out, void* stream);
 
+/* Training sample batches generated on the device, replacing train.py:34-61
+   (sample_mesh_points: random tetrahedron uniform over cells, sorted-uniform barycentric
+   weights), :273-282 (ground truth through gpu_sampleu) and :286-315 (per-batch 21-bit
+   Morton sort, clamped to [0,1]).  Mesh: pts [npts][3] float32, conn4 [C][4] int32 vertex
+   ids in [0, npts), values [npts] float64, all device pointers.  Output: samples_out
+   [num_batches][batch_size][3] float32, each batch sorted stably by its 63-bit Morton
+   code, and gt_out [num_batches][batch_size] float32, the point field interpolated at each
+   sample by the tetrahedral locator (lowest containing cell, -1 outside), or NULL to skip
+   it.  Random numbers: Philox4x32-10 keyed by `seed`, so the same seed gives the same
+   batches on every device.  num_batches * batch_size must stay below 2^31 - 4096. */
+int gvc_training_samples(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, const int32_t* conn4,
+                         const double* values, int64_t num_batches, int64_t batch_size, uint64_t seed,
+                         float* samples_out, float* gt_out, void* stream);
+
 /* No counterpart in the reference.  Tetrahedral sampling for callers that cannot
    allocate device memory (their memory belongs to another allocator, or cudaMalloc's
    device-wide synchronisation is unacceptable where they call).  Same inputs, outputs

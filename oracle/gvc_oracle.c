@@ -1294,3 +1294,53 @@ void orc_knn3_mean_dist2(int64_t n, const float* pts, float* out, int nthreads) 
     free(cellof);
     free(items);
 }
+
+/* ------------------------------------------------------------------------------------
+ * Training sample points (train.py:34-61 sample_mesh_points), with the device's
+ * declared generator: Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC 2011), counter =
+ * (point index lo, hi, block, 0), key = (seed lo, seed hi).  Block 0 gives the cell
+ * (floor(r64 * C / 2^64), r64 = word0:word1) and two uniforms (words 2, 3), block 1
+ * word 0 the third; a uniform is (r >> 8) * 2^-24.  The three are sorted and their gaps
+ * (u0, u1 - u0, u2 - u1, 1 - u2) weight the tetrahedron's vertices, summed left to right
+ * in float32 with every operation rounded.
+ * ------------------------------------------------------------------------------------ */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; r++) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n1 = (uint32_t)p1;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1, n3 = (uint32_t)p0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static inline float unit24f(uint32_t r) { return (float)(r >> 8) * 5.9604644775390625e-8f; }
+
+void orc_tet_points(int64_t N, uint64_t seed, const float* pts, const int64_t* conn4, int64_t C, float* out,
+                    int nthreads) {
+    int nt = orc_nthreads(nthreads);
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t t = 0; t < N; t++) {
+        uint32_t ca[4] = {(uint32_t)t, (uint32_t)((uint64_t)t >> 32), 0u, 0u}, a[4];
+        uint32_t cb[4] = {(uint32_t)t, (uint32_t)((uint64_t)t >> 32), 1u, 0u}, b[4];
+        orc_philox4x32_10(ca, key, a);
+        orc_philox4x32_10(cb, key, b);
+        uint64_t r64 = ((uint64_t)a[0] << 32) | a[1];
+        int64_t cell = (int64_t)(((unsigned __int128)r64 * (unsigned __int128)(uint64_t)C) >> 64);
+        float u[3] = {unit24f(a[2]), unit24f(a[3]), unit24f(b[0])};
+        for (int i = 1; i < 3; i++)
+            for (int j = i; j > 0 && u[j] < u[j - 1]; j--) { float tmp = u[j]; u[j] = u[j - 1]; u[j - 1] = tmp; }
+        float w[4] = {u[0], u[1] - u[0], u[2] - u[1], 1.0f - u[2]};
+        const int64_t* cv = conn4 + 4 * cell;
+        for (int ax = 0; ax < 3; ax++) {
+            float s = w[0] * pts[3 * cv[0] + ax];
+            s = s + w[1] * pts[3 * cv[1] + ax];
+            s = s + w[2] * pts[3 * cv[2] + ax];
+            s = s + w[3] * pts[3 * cv[3] + ax];
+            out[3 * t + ax] = s;
+        }
+    }
+}

@@ -60,6 +60,8 @@ def lib():
             "orc_tet_boxes": [i64, vp, vp, vp],
             "orc_sample_cells": [i64, vp, i64, vp, vp, vp, vp, i64, vp, vp, vp, i32],
             "orc_knn3_mean_dist2": [i64, vp, vp, i32],
+            "orc_philox4x32_10": [vp, vp, vp],
+            "orc_tet_points": [i64, ctypes.c_uint64, vp, vp, i64, vp, i32],
             "orc_openmp_enabled": [],
         }
         for name, args in sig.items():
@@ -245,6 +247,35 @@ def knn3_mean_dist2(pts, nthreads=0):
     out = np.zeros(pts.shape[0], np.float32)
     lib().orc_knn3_mean_dist2(pts.shape[0], _p(pts), _p(out), nthreads)
     return out
+
+
+def philox4x32_10(ctr, key):
+    """Philox4x32-10 of one counter block (four uint32) under a key (two uint32)."""
+    c = _c(ctr, np.uint32)
+    k = _c(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib().orc_philox4x32_10(_p(c), _p(k), _p(out))
+    return out
+
+
+def training_samples(pts, tets, values, num_batches, batch_size, seed=0, nthreads=0):
+    """Training batches of train.py:34-61 + :273-315 with the declared Philox generator:
+    points in random tetrahedra, per-batch stable sort by the clamped 21-bit Morton code
+    (morton21, pinned to the reference's own code), ground truth by the tetrahedral
+    locator at the sorted points, converted to float32.  Returns ([B,S,3], [B,S])."""
+    pts = _c(pts, np.float32).reshape(-1, 3)
+    tets = _c(tets, np.int64).reshape(-1, 4)
+    N = num_batches * batch_size
+    raw = np.zeros((N, 3), np.float32)
+    lib().orc_tet_points(N, int(seed), _p(pts), _p(tets), tets.shape[0], _p(raw), nthreads)
+    keys = morton21(raw, clamp=True).reshape(num_batches, batch_size)
+    order = np.argsort(keys, axis=1, kind="stable")
+    samples = np.take_along_axis(raw.reshape(num_batches, batch_size, 3), order[:, :, None], axis=1)
+    gt = None
+    if values is not None:
+        v, _ = sample_tets(pts, tets, values, samples.reshape(-1, 3), nthreads)
+        gt = v.astype(np.float32).reshape(num_batches, batch_size)
+    return samples, gt
 
 
 # --------------------------------------------------------------------------------------
