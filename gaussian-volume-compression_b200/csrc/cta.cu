@@ -649,18 +649,20 @@ __global__ void __launch_bounds__((4 / RPT) * 32 + 32,
                     mm &= mm - 1;
                     const float4 lo = sm.gd[stage][j][3], hi = sm.gd[stage][j][4];
                     bool inr[RPT];
-                    bool anyin = false;
+                    uint32_t kany = 0;
 #pragma unroll
                     for (int k = 0; k < RPT; k++) {
                         const float x = xr[k], y = yr[k], z = zr[k];
                         inr[k] = ing[k] && lo.x <= x && x <= hi.x && lo.y <= y && y <= hi.y && lo.z <= z && z <= hi.z;
-                        anyin |= inr[k];
+                        kany |= __any_sync(0xffffffffu, inr[k]) ? (1u << k) : 0u;
                     }
-                    // the column's box overlaps the warp's rows, but often no row lies inside it
-                    if (!__any_sync(0xffffffffu, anyin)) continue;
+                    // the column's box overlaps the warp's rows, but often no row lies inside it; a
+                    // vote per row chain also skips the chain none of whose rows is inside
+                    if (!kany) continue;
                     const float4 r0 = sm.gd[stage][j][0], r1 = sm.gd[stage][j][1], r2 = sm.gd[stage][j][2];
 #pragma unroll
                     for (int k = 0; k < RPT; k++) {
+                        if (!((kany >> k) & 1u)) continue;
                         const float x = xr[k], y = yr[k], z = zr[k];
                         const bool in = inr[k];
                         const float dx = x - r0.x, dy = y - r0.y, dz = z - r0.z;
