@@ -199,7 +199,8 @@ def sample_training_batches(pts_arr, tets_arr, val_arr, num_batches, batch_size,
     the ground truth.  gt_cells = (conn, cell_types, cell_offsets) takes the ground truth
     from that (untriangulated) cell mesh instead, as the reference does when it samples
     the original mesh.  Returns CUDA tensors (samples [B,S,3] float32, gt [B,S] float32);
-    nothing goes through host memory after the mesh upload.
+    nothing goes through host memory after the mesh upload.  The call's workspace (about
+    48 bytes per sample) belongs to a context of its own, released before returning.
     """
     pts = np.ascontiguousarray(pts_arr, dtype=np.float32).reshape(-1, 3)
     tets = np.ascontiguousarray(tets_arr, dtype=np.int64).reshape(-1, 4)
@@ -213,7 +214,8 @@ def sample_training_batches(pts_arr, tets_arr, val_arr, num_batches, batch_size,
         raise RuntimeError("connectivity refers to a point outside the point array")
     if vals.size < pts.shape[0]:
         raise RuntimeError("values must hold one entry per point")
-    dev, c = _ctx()
+    dev = torch.cuda.current_device()
+    c = _n.Context()   # one-off workspace, freed with the context at the end of the call
     d = "cuda:%d" % dev
     samples = torch.empty((B, S, 3), dtype=torch.float32, device=d)
     gt = torch.empty((B, S), dtype=torch.float32, device=d)

@@ -172,7 +172,8 @@ int gvc_knn3_mean_dist2(gvc_ctx* ctx, int64_t n, const float* pts, float* out, v
    code, and gt_out [num_batches][batch_size] float32, the point field interpolated at each
    sample by the tetrahedral locator (lowest containing cell, -1 outside), or NULL to skip
    it.  Random numbers: Philox4x32-10 keyed by `seed`, so the same seed gives the same
-   batches on every device.  num_batches * batch_size must stay below 2^31 - 4096. */
+   batches on every device.  num_batches * batch_size must stay below 2^31 - 4096.  The
+   workspace (about 48 bytes per sample) stays with the context until gvc_ctx_destroy. */
 int gvc_training_samples(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C, const int32_t* conn4,
                          const double* values, int64_t num_batches, int64_t batch_size, uint64_t seed,
                          float* samples_out, float* gt_out, void* stream);
