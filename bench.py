@@ -480,7 +480,8 @@ def run_ours(args):
                 "frac": achieved / bf16, "traffic": traffic, "kernel": name, "kernel_ms": t_k,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size launch"
                                   if traffic else None,
-                "peak_source": "%s bf16 dense (MEASURED_PEAKS.json)" % src,
+                "peak_source": ("measured bf16 dense burst (MEASURED_PEAKS.json)" if src == "measured" else
+                                "fallback bf16 dense 1.59 PFLOP/s (MEASURED_PEAKS.json absent)"),
                 "fp32_simt_nominal_tflops": FP32_NOMINAL_TFLOPS,
                 "frac_of_fp32_simt_nominal": achieved / FP32_NOMINAL_TFLOPS,
                 "fwd_kernel_ms": t_fwd, "bwd_kernel_ms": t_bwd,
