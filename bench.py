@@ -498,18 +498,26 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e and not args.profile:
         h_samples = torch.from_numpy(samples).pin_memory()
+        # the target values travel with their samples, as the training loop's sorted
+        # (samples, ground truth) batches do (train.py:286-315)
+        h_gt = target_field(torch.from_numpy(samples)).pin_memory()
         h_params = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
                     for a in (means, scales, rots, values.reshape(-1, 1), weights.reshape(-1, 1))]
         settings = R.GaussianRasterizationSettings((0, 0, 0), (1, 1, 1), 0, -1.0, 1.0, ugb, False)
         rast = R.GaussianRasterizer(settings)
-        h2d = h_samples.numel() * 4 + sum(p.numel() * 4 for p in h_params)
+        h2d = h_samples.numel() * 4 + h_gt.numel() * 4 + sum(p.numel() * 4 for p in h_params)
 
         # double-buffered uploads: the inputs of step k + 1 are copied on a second stream
         # while step k computes (every step's copy is inside the timed region)
         copy_stream = torch.cuda.Stream(dev)
-        hosts = [h_samples] + h_params
+        hosts = [h_samples, h_gt] + h_params
         bufs = [[torch.empty(h.shape, dtype=h.dtype, device=dev) for h in hosts] for _ in range(2)]
         ready = [torch.cuda.Event(), torch.cuda.Event()]
+        # each step's loss lands in pinned memory; the host reads step k's value after step
+        # k + 1 is queued, so the GPU is not idle while the host reads
+        h_loss = [torch.zeros(1, dtype=torch.float32).pin_memory() for _ in range(2)]
+        loss_done = [torch.cuda.Event(), torch.cuda.Event()]
+        losses = []
 
         def issue_copy(b):
             copy_stream.wait_stream(stream)  # the buffer's previous step has finished with it
@@ -523,23 +531,28 @@ def run_ours(args):
             stream.wait_event(ready[b])
             if k + 1 < n:
                 issue_copy(1 - b)
-            s_d = bufs[b][0]
-            leaves = [p.detach().requires_grad_(True) for p in bufs[b][1:]]
+            s_d, gt = bufs[b][0], bufs[b][1]
+            leaves = [p.detach().requires_grad_(True) for p in bufs[b][2:]]
             rast.build_bvh(s_d)
             cells, cw = rast(leaves[0], leaves[1], leaves[2], leaves[3], leaves[4])
-            gt = target_field(s_d)
             # masked mean without boolean indexing (no device-to-host size query)
             mask = ((cells != -1) & (gt != -1)).float()
             loss = (torch.abs(cells - gt) * mask).sum() / mask.sum().clamp_min(1.0)
             loss.backward()
             if world > 1:
                 gvc_dist.allreduce_grads([l.grad for l in leaves])
-            return loss.item()
+            h_loss[b].copy_(loss.detach().reshape(1), non_blocking=True)
+            loss_done[b].record(stream)
+            if k > 0:  # the previous step's result, read while this step runs
+                loss_done[1 - b].synchronize()
+                losses.append(float(h_loss[1 - b][0]))
 
         def e2e_run(n):
             issue_copy(0)
             for k in range(n):
                 e2e_step(k, n)
+            loss_done[(n - 1) % 2].synchronize()
+            losses.append(float(h_loss[(n - 1) % 2][0]))
 
         e2e_run(max(1, args.warmup))
         torch.cuda.synchronize()
@@ -553,8 +566,10 @@ def run_ours(args):
         torch.cuda.synchronize()
         e2e_ms = gvc_dist.max_over_ranks(a0.elapsed_time(a1) / n_e2e, dev)
         e2e = {"value": e2e_ms, "unit": "ms/step", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4,
-               "steps": n_e2e, "path": "GaussianRasterizer (autograd) + masked L1 + loss.item(); "
-                                         "pinned host inputs uploaded every step, double-buffered on a copy stream"}
+               "steps": n_e2e, "last_loss": losses[-1],
+               "path": "GaussianRasterizer (autograd) + masked L1; every step uploads its pinned host inputs "
+                       "(samples, their target values, parameters; double-buffered on a copy stream) and "
+                       "reads its loss back to pinned host memory (checked on the host while the next step runs)"}
 
     # the two evaluation paths side by side: full step time and forward outputs (kept on the
     # host for the FP64 comparison below)
