@@ -87,3 +87,19 @@ def test_sampleu_mixed_vtk_arrays(cuda, orc):
     ref, _ = orc.sample_cells(pts, types, offs[:-1], conn, vals, q)
     assert out.dtype == np.float64
     np.testing.assert_array_equal(out, ref)
+
+
+@pytest.mark.parametrize("n", [2, 4])
+def test_tets_shared_faces_bit_exact(cuda, orc, n):
+    """Points exactly on faces shared by several tetrahedra: the lowest containing cell
+    wins on the GPU as in the oracle."""
+    from gpu_mesh_sampling._gpu_mesh_sampling import sample_meshu_cells
+    from test_mesh_oracle import face_points
+    pts, tets = orc.jittered_tet_mesh(n=n, seed=0, jitter=0.0)
+    vals = orc.blob_field(pts).astype(np.float64)
+    q = face_points(n)
+    out, cell = sample_meshu_cells(pts, tets, vals, q)
+    ref, rcell = orc.sample_tets(pts, tets, vals, q)
+    np.testing.assert_array_equal(cell, rcell)
+    np.testing.assert_array_equal(out, ref)
+    assert (cell >= 0).all()

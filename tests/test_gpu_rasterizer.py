@@ -360,3 +360,27 @@ def test_large_clustered_properties(cuda, orc):
     a, *_ = run_backward(cuda, case, gout, gw, "deterministic")
     b, *_ = run_backward(cuda, case, gout, gw, "atomic")
     assert_grads_close(b, a, tol=1e-4, cov_tol=1e-3)
+
+
+@pytest.mark.parametrize("path", ["plain", "tensor_core", "plain_tile"])
+def test_power_window_at_minus_14(cuda, orc, path):
+    """Pairs just inside (-13.98) and just outside (-14.02) the power floor of
+    forward.cu:235, inside the pair's box: only the first adds w e^p to W."""
+    from bvh_diff_gaussian_rasterization import _C
+    from test_oracle import window_case, window_points
+    case = window_case()
+    means, scales, rots, values, weights = case
+    x, powers, _, _ = window_points(orc, case)
+    _C.set_eval_path(path)
+    try:
+        out, outw, conics = run_forward(cuda, means, scales, rots, values, weights, x)
+    finally:
+        _C.set_eval_path("plain")
+    outw = outw.cpu().numpy().astype(np.float64)
+    gc = conics.cpu().numpy().reshape(-1, 6).astype(np.float64)
+    _, gb = gpu_preprocess(gvc_native.Context(), cuda, means, scales, rots, weights)
+    _, w_wide = orc.forward(means[1:], values[1:], weights[1:], gc[1:], gb[1:], x)
+    pair = outw - w_wide
+    expect = np.where(powers >= -14.0, 0.9 * np.exp(powers), 0.0)
+    assert np.all(outw > 0.01)
+    np.testing.assert_allclose(pair, expect, rtol=1e-3, atol=1e-7)

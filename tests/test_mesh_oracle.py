@@ -122,3 +122,34 @@ def test_cells_zero_volume_types_and_tet_agreement(orc):
     types = np.array([1, 3, 5], np.uint8)
     out, cell = orc.sample_cells(pts, types, np.array([0, 1, 3]), conn, vals, pts[:50])
     assert (cell == -1).all() and (out == -1.0).all()
+
+
+def face_points(n=2):
+    """Points exactly on faces shared by two or more tetrahedra of an unjittered n^3 Kuhn
+    grid: on the grid planes between hexahedra and on the diagonal planes inside each
+    hexahedron (dyadic coordinates, so every orientation test is exact)."""
+    h = 1.0 / n
+    pts = []
+    for a in range(1, n):
+        for y in (0.25, 0.375, 0.625):
+            for z in (0.125, 0.3125, 0.875):
+                pts.append([a * h, y, z])
+                pts.append([y, a * h, z])
+                pts.append([z, y, a * h])
+    for v in (0.125, 0.25, 0.375):
+        pts.append([v, v, 0.0625])       # on x = y inside the first hexahedron
+        pts.append([v, 0.03125, v])      # on x = z
+        pts.append([0.03125, v, v])      # on y = z
+    return np.array(pts, np.float32)
+
+
+def test_tets_lowest_id_on_shared_face(orc):
+    pts, tets = orc.jittered_tet_mesh(n=2, seed=0, jitter=0.0)
+    vals = np.arange(pts.shape[0], dtype=np.float64)
+    q = face_points(2)
+    out, cell = orc.sample_tets(pts, tets, vals, q)
+    for i in range(q.shape[0]):
+        owners = [c for c in range(tets.shape[0])
+                  if orc.sample_tets(pts, tets[c:c + 1], vals, q[i:i + 1])[1][0] == 0]
+        assert len(owners) >= 2, (i, q[i], owners)   # the point is on a shared face
+        assert cell[i] == min(owners)

@@ -236,3 +236,46 @@ def test_morton_keys_known_answers(orc):
     pts = np.array([[0, 0, 0], [1, 1, 1], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32)
     keys, skeys, perm = orc.morton30_points(pts)
     assert keys.tolist() == [0, (1 << 30) - 1, 0x09249249, 0x09249249 << 1, 0x09249249 << 2]
+
+
+def window_case():
+    """An elongated Gaussian turned 45 degrees about z, whose box (built from the rows of the
+    rotation, forward.cu:91-112) reaches far past its ellipsoid, plus a wide isotropic one
+    that keeps W above the 0.01 cutoff; points on the first one's minor axis at powers
+    -13.98, -14.02 (either side of the -14 floor, forward.cu:235), -10 and -20."""
+    c, s = np.cos(np.pi / 8), np.sin(np.pi / 8)
+    means = np.array([[0.5, 0.5, 0.5], [0.5, 0.5, 0.5]], np.float32)
+    scales = np.array([[0.2, 0.004, 0.004], [0.3, 0.3, 0.3]], np.float32)
+    rots = np.array([[c, 0, 0, s], [1, 0, 0, 0]], np.float32)
+    weights = np.array([0.9, 0.05], np.float32)
+    values = np.array([0.2, 0.7], np.float32)
+    return means, scales, rots, values, weights
+
+
+def window_points(orc, case):
+    means, scales, rots, values, weights = case
+    _, c64, bb = orc.preprocess(means, scales, rots, weights)
+    C = np.array([[c64[0, 0], c64[0, 1], c64[0, 2]], [c64[0, 1], c64[0, 3], c64[0, 4]],
+                  [c64[0, 2], c64[0, 4], c64[0, 5]]])
+    u = np.linalg.eigh(C)[1][:, -1]  # minor axis of the elongated Gaussian
+    powers = np.array([-13.98, -14.02, -10.0, -20.0])
+    t = np.sqrt(-2 * powers / (u @ C @ u))
+    x = (means[0][None, :].astype(np.float64) + t[:, None] * u[None, :]).astype(np.float32)
+    return x, powers, c64, bb
+
+
+def test_power_window_bounds(orc):
+    case = window_case()
+    means, scales, rots, values, weights = case
+    x, powers, c64, bb = window_points(orc, case)
+    assert np.all((x >= bb[0, :3]) & (x <= bb[0, 3:]))  # every point inside the first box
+    _, outw = orc.forward(means, values, weights, c64, bb, x)
+    _, w_wide = orc.forward(means[1:], values[1:], weights[1:], c64[1:], bb[1:], x)
+    pair = outw - w_wide
+    d = x.astype(np.float64) - means[0]
+    C = np.array([[c64[0, 0], c64[0, 1], c64[0, 2]], [c64[0, 1], c64[0, 3], c64[0, 4]],
+                  [c64[0, 2], c64[0, 4], c64[0, 5]]])
+    p = -0.5 * np.einsum("ni,ij,nj->n", d, C, d)
+    expect = np.where(p >= -14.0, 0.9 * np.exp(p), 0.0)
+    np.testing.assert_allclose(pair, expect, rtol=1e-6, atol=1e-11)
+    assert pair[0] > 0 and pair[1] == 0 and pair[2] > 0 and pair[3] == 0
