@@ -63,7 +63,7 @@ struct CtaArgs {
 // Block groups split where both halves' boxes have at most `ratio` of the whole's
 // half-perimeter: kBlockSplitForward for the forward, kBlockSplitBackward (finer) for the
 // tensor-core backward.
-constexpr float kBlockSplitForward = 0.5f;
+constexpr float kBlockSplitForward = 0.45f;
 constexpr float kBlockSplitBackward = 0.65f;
 cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32_t* skeys, uint2* bdesc,
                                  float4* bboxes, float ratio, cudaStream_t st);
