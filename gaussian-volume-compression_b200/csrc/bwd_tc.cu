@@ -28,7 +28,7 @@ namespace gvc {
 constexpr int kBRows = 128;            // sample rows per block (the forward's blocks)
 constexpr int kBGroups = 8;            // block groups per block
 constexpr int kBBatch = 128;           // candidate Gaussians per batch (consumer threads)
-constexpr int kBStages = 2;            // candidate batches in flight
+constexpr int kBStages = 4;            // candidate batches in flight
 constexpr int kBChunks = kBRows / 16;  // K chunks of 16 rows
 constexpr int kMom = 32;               // B rows: 20 moment features + zero padding
 

@@ -451,7 +451,7 @@ struct Producer {
 // (48 warps, 40 registers).
 constexpr int kCtaMinBlocksTc = 6;
 constexpr int kCtaMinBlocksSimt1 = 8;
-constexpr int kCtaMinBlocksSimt2 = 16;
+constexpr int kCtaMinBlocksSimt2 = 14;
 // Rows per consumer thread of the SIMT variant: each staged record (80 bytes broadcast to
 // every lane) then serves two samples, halving the shared-memory datapath traffic.
 constexpr int kSimtRowsPerThread = 2;
