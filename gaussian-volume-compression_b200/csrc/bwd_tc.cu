@@ -142,7 +142,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
         sm.rows[t] = p;
     }
     if (w == 0) {
-        tmem_alloc(&sm.tmem_base, 32);
+        static_assert(tmem_cols_ok(kMom), "TMEM columns must be a power of two >= 32");
+        tmem_alloc(&sm.tmem_base, kMom);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (w == 0) tmem_dealloc(tmem, 32);
+    if (w == 0) tmem_dealloc(tmem, kMom);
 }
 
 template <bool COUNT>

@@ -467,6 +467,7 @@ __global__ void __launch_bounds__((4 / RPT) * 32 + 32,
     CtaSmem<TC>& sm = *reinterpret_cast<CtaSmem<TC>*>(smem_raw);
     static_assert(!TC || RPT == 1, "the tensor-core variant owns one row (TMEM lane) per thread");
     constexpr int kStages = kStagesOf<TC>;
+    static_assert(!TC || tmem_cols_ok(kStages * kBatch), "TMEM columns must be a power of two >= 32");
     constexpr int NCW = 4 / RPT;  // consumer warps; warp NCW is the producer
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int64_t blk = blockIdx.x;

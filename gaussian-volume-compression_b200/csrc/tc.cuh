@@ -62,6 +62,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int* st
 
 // ---- tensor memory --------------------------------------------------------------------
 // Warp-wide: allocates ncols (power of 2, >= 32) columns; the TMEM address goes to *dst.
+// A TMEM allocation is a power of two of at least 32 columns (anything else is an
+// illegal instruction); callers check their column counts with this at compile time.
+__host__ __device__ constexpr bool tmem_cols_ok(uint32_t n) { return n >= 32 && n <= 512 && (n & (n - 1)) == 0; }
+
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)),
                  "r"(ncols)
