@@ -384,3 +384,25 @@ def test_power_window_at_minus_14(cuda, orc, path):
     expect = np.where(powers >= -14.0, 0.9 * np.exp(powers), 0.0)
     assert np.all(outw > 0.01)
     np.testing.assert_allclose(pair, expect, rtol=1e-3, atol=1e-7)
+
+
+@pytest.mark.parametrize("path", ["plain", "tensor_core", "plain_tile"])
+def test_weight_cutoff_known_answer(cuda, orc, path):
+    """One isotropic Gaussian sampled at its mean: W = w just above the 0.01 cutoff gives
+    out = v, outw = w; just below gives out = -1, outw = 0 (config.h:9,
+    forward.cu:250-256)."""
+    from bvh_diff_gaussian_rasterization import _C
+    m = np.array([[0.5, 0.5, 0.5]], np.float32)
+    s = np.array([[0.05, 0.05, 0.05]], np.float32)
+    q = np.array([[1, 0, 0, 0]], np.float32)
+    v = np.array([0.3], np.float32)
+    x = np.repeat(m, 33, 0)  # a partial tile of samples all at the mean
+    _C.set_eval_path(path)
+    try:
+        for w, expect in ((0.0101, 0.3), (0.0099, -1.0)):
+            out, outw, _ = run_forward(cuda, m, s, q, v, np.array([w], np.float32), x)
+            out, outw = out.cpu().numpy(), outw.cpu().numpy()
+            np.testing.assert_allclose(out, expect, rtol=1e-6)
+            np.testing.assert_allclose(outw, w if expect > 0 else 0.0, rtol=1e-6)
+    finally:
+        _C.set_eval_path("plain")
