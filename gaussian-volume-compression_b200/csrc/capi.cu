@@ -316,9 +316,19 @@ int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int 
         const int64_t n_blocks = (S + 127) / 128;
         GVC_CUDA(ctx->blk_desc.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc");
         GVC_CUDA(ctx->blk_boxes.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes");
+        // when the options already select the tensor-core backward, its finer block groups
+        // come from the same launch; otherwise that backward builds them on first use
+        const bool tc_bwd = ctx->bwd_mode == 3 || (ctx->bwd_mode == 0 && ctx->eval_path == 1);
+        if (tc_bwd) {
+            GVC_CUDA(ctx->blk_desc_b.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc_b");
+            GVC_CUDA(ctx->blk_boxes_b.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes_b");
+        }
         GVC_CUDA(launch_sample_blocks(S, ctx->s_sorted.as<float4>(), ctx->s_sort.keys.as<uint32_t>(),
-                                      ctx->blk_desc.as<uint2>(), ctx->blk_boxes.as<float4>(), kBlockSplitForward, st),
+                                      ctx->blk_desc.as<uint2>(), ctx->blk_boxes.as<float4>(), kBlockSplitForward, st,
+                                      tc_bwd ? ctx->blk_desc_b.as<uint2>() : nullptr,
+                                      tc_bwd ? ctx->blk_boxes_b.as<float4>() : nullptr, kBlockSplitBackward),
                  "sample blocks");
+        ctx->blk_b_ready = tc_bwd;
     }
     ctx->samples_ready = true;
     tm.mark();

@@ -120,37 +120,15 @@ __device__ int rows_split(int a, int b, const uint32_t* keys, const uint32_t (&k
 
 constexpr int kBlocksPerCta = 8;  // 128-row blocks (warps) per CTA of k_sample_blocks
 
-// bdesc[blk] = (starts of groups 1..7 as bytes, 128 if unused; byte 7 = group count);
-// bboxes[blk * 8 + g] = (lo, hi) of group g (empty box if unused).  The range [0, nvalid)
-// is split three times (every range of a level in order), giving at most 8 groups.
-__global__ void __launch_bounds__(32 * kBlocksPerCta) k_sample_blocks(const float4* __restrict__ s_sorted,
-                                                                      const uint32_t* __restrict__ skeys, int64_t S,
-                                                                      int64_t n_blocks, uint2* __restrict__ bdesc,
-                                                                      float4* __restrict__ bboxes, float ratio) {
-    __shared__ uint32_t s_keys[kBlocksPerCta][kBlockRows];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t blk = (int64_t)blockIdx.x * kBlocksPerCta + warp;
-    if (blk >= n_blocks) return;
-    uint32_t* keys = s_keys[warp];
-    float x[4], y[4], z[4];
-    uint32_t key[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int64_t row = blk * kBlockRows + 4 * lane + k;
-        x[k] = y[k] = z[k] = NAN;
-        key[k] = 0xffffffffu;
-        if (row < S) {
-            const float4 p = s_sorted[row];
-            x[k] = p.x;
-            y[k] = p.y;
-            z[k] = p.z;
-            key[k] = skeys[row];
-        }
-        keys[4 * lane + k] = key[k];
-    }
-    __syncwarp();
-    const int64_t rem = S - blk * kBlockRows;
-    const int nvalid = rem < kBlockRows ? (int)rem : kBlockRows;
+// Splits the block's valid rows [0, nvalid) three times (every range of a level in
+// order, at most 8 groups) with `ratio` and writes bdesc[blk] = (starts of groups 1..7
+// as bytes, 128 if unused; byte 7 = group count) and bboxes[blk * 8 + g] = (lo, hi) of
+// group g (empty box if unused).
+__device__ __forceinline__ void block_split_store(int64_t blk, int nvalid, const uint32_t* keys,
+                                                  const uint32_t (&key)[4], const float (&x)[4],
+                                                  const float (&y)[4], const float (&z)[4], float ratio,
+                                                  uint2* __restrict__ bdesc, float4* __restrict__ bboxes) {
+    const int lane = threadIdx.x & 31;
     int ra[kBlockGroups], rb[kBlockGroups];
     int nr = 1;
     ra[0] = 0;
@@ -192,6 +170,42 @@ __global__ void __launch_bounds__(32 * kBlocksPerCta) k_sample_blocks(const floa
         d.y = starts[5] | (starts[6] << 8) | (starts[7] << 16) | ((uint32_t)nr << 24);
         bdesc[blk] = d;
     }
+}
+
+// One warp per 128-row block: the rows are loaded once and split with `ratio` into
+// (bdesc, bboxes) and, when bdesc2 is given, also with `ratio2` into (bdesc2, bboxes2).
+__global__ void __launch_bounds__(32 * kBlocksPerCta) k_sample_blocks(const float4* __restrict__ s_sorted,
+                                                                      const uint32_t* __restrict__ skeys, int64_t S,
+                                                                      int64_t n_blocks, uint2* __restrict__ bdesc,
+                                                                      float4* __restrict__ bboxes, float ratio,
+                                                                      uint2* __restrict__ bdesc2,
+                                                                      float4* __restrict__ bboxes2, float ratio2) {
+    __shared__ uint32_t s_keys[kBlocksPerCta][kBlockRows];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t blk = (int64_t)blockIdx.x * kBlocksPerCta + warp;
+    if (blk >= n_blocks) return;
+    uint32_t* keys = s_keys[warp];
+    float x[4], y[4], z[4];
+    uint32_t key[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int64_t row = blk * kBlockRows + 4 * lane + k;
+        x[k] = y[k] = z[k] = NAN;
+        key[k] = 0xffffffffu;
+        if (row < S) {
+            const float4 p = s_sorted[row];
+            x[k] = p.x;
+            y[k] = p.y;
+            z[k] = p.z;
+            key[k] = skeys[row];
+        }
+        keys[4 * lane + k] = key[k];
+    }
+    __syncwarp();
+    const int64_t rem = S - blk * kBlockRows;
+    const int nvalid = rem < kBlockRows ? (int)rem : kBlockRows;
+    block_split_store(blk, nvalid, keys, key, x, y, z, ratio, bdesc, bboxes);
+    if (bdesc2) block_split_store(blk, nvalid, keys, key, x, y, z, ratio2, bdesc2, bboxes2);
 }
 
 __device__ __forceinline__ int group_start(uint2 d, int g) {
@@ -723,11 +737,12 @@ __global__ void __launch_bounds__((4 / RPT) * 32 + 32,
 static inline unsigned nblk128(int64_t n) { return (unsigned)((n + kBlockRows - 1) / kBlockRows); }
 
 cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32_t* skeys, uint2* bdesc,
-                                 float4* bboxes, float ratio, cudaStream_t st) {
+                                 float4* bboxes, float ratio, cudaStream_t st, uint2* bdesc2, float4* bboxes2,
+                                 float ratio2) {
     if (S <= 0) return cudaSuccess;
     const int64_t nb = (S + kBlockRows - 1) / kBlockRows;
     k_sample_blocks<<<(unsigned)((nb + kBlocksPerCta - 1) / kBlocksPerCta), 32 * kBlocksPerCta, 0, st>>>(
-        s_sorted, skeys, S, nb, bdesc, bboxes, ratio);
+        s_sorted, skeys, S, nb, bdesc, bboxes, ratio, bdesc2, bboxes2, ratio2);
     gvc::note_launch();
     return cudaGetLastError();
 }

@@ -65,8 +65,11 @@ struct CtaArgs {
 // tensor-core backward.
 constexpr float kBlockSplitForward = 0.45f;
 constexpr float kBlockSplitBackward = 0.65f;
+// Block groups with `ratio`; with bdesc2 also a second set with `ratio2` from the same
+// loaded rows (one launch).
 cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32_t* skeys, uint2* bdesc,
-                                 float4* bboxes, float ratio, cudaStream_t st);
+                                 float4* bboxes, float ratio, cudaStream_t st, uint2* bdesc2 = nullptr,
+                                 float4* bboxes2 = nullptr, float ratio2 = 0.f);
 cudaError_t launch_forward_cta(const CtaArgs& a, bool tc, cudaStream_t st);
 cudaError_t launch_tc_gemm_test(const void* A, const void* B, int N, float* D, int* status, cudaStream_t st);
 cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st);
