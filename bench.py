@@ -43,6 +43,8 @@ CONFIGS = {
     "small": (200_000, 2_000_000, "profiling case: 200k clustered Gaussians x 2M points"),
     "slice": (2_000_000, 4_000_000, "profiling case with the large evaluation's Gaussians: 2M clustered Gaussians x 4M points"),
     "tiny": (4_096, 262_144, "CPU-runnable case: 4096 clustered Gaussians x 64^3 points"),
+    "config1": (4_096, 262_144, "small mixture: 4096 Gaussians (means U[0,1]^3, log-scales N(log 0.02, 0.3)) "
+                                "at the 64^3 cell centres"),
 }
 METRIC = "fwd+bwd ms/step (2M Gaussians×16M pts), TC vs plain FP32 at stated FP64 err"
 # Algorithmic FP32 work per pair (FORWARD forward.cu:224-256, BACKWARD backward.cu:252-298):
@@ -89,6 +91,9 @@ def parse():
 def workload(cfg, rank):
     import gvc_workloads as wl
     P, S, desc = CONFIGS[cfg]
+    if cfg == "config1":
+        means, scales, rots, values, weights = wl.mixture_small(seed=0, P=P)
+        return means, scales, rots, values, weights, wl.grid_centres(64), desc
     means, scales, rots, values, weights, _ = wl.mixture_large(seed=0, P=P, S=2)
     # per-rank sample set (weak scaling); rank 0 uses the config's own seed
     _, _, _, _, _, samples = wl.mixture_large(seed=0 if rank == 0 else 1000 + rank, P=P, S=S)
