@@ -128,9 +128,6 @@ __global__ void __launch_bounds__(256) k_keys(Src src, int64_t n, const uint32_t
 //   k_rs_scan (per-digit exclusive scan over blocks + digit totals),
 //   k_rs_scatter (stable ranks: (warp, iteration, lane) = input order).
 // ----------------------------------------------------------------------------------
-constexpr int kRsWarps = 8;
-constexpr int kRsIters = 16;
-constexpr int kRsTile = kRsWarps * kRsIters * 32;
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -309,10 +306,10 @@ cudaError_t radix_sort_pairs(Lbvh& L, int64_t n, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const int nb = (int)((n + kRsTile - 1) / kRsTile);
     cudaError_t e;
-    if ((e = L.keys_alt.ensure(sizeof(uint32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.perm.ensure(sizeof(int32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.perm_alt.ensure(sizeof(int32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.hist.ensure(sizeof(uint32_t) * (256 * (size_t)nb + 256))) != cudaSuccess) return e;
+    if ((e = L.keys_alt.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.perm.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.perm_alt.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.hist.ensure(LbvhBytes::hist(n))) != cudaSuccess) return e;
     uint32_t* hist = L.hist.as<uint32_t>();
     uint32_t* totals = hist + 256 * (size_t)nb;
     uint32_t* kin = L.keys.as<uint32_t>();
@@ -345,10 +342,10 @@ cudaError_t radix_sort_words(Lbvh& L, int64_t n, const uint32_t* const* words, c
     const int nb = (int)((n + kRsTile - 1) / kRsTile);
     cudaError_t e;
     if ((e = L.keys.ensure(sizeof(uint32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.keys_alt.ensure(sizeof(uint32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.perm.ensure(sizeof(int32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.perm_alt.ensure(sizeof(int32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.hist.ensure(sizeof(uint32_t) * (256 * (size_t)nb + 256))) != cudaSuccess) return e;
+    if ((e = L.keys_alt.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.perm.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.perm_alt.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.hist.ensure(LbvhBytes::hist(n))) != cudaSuccess) return e;
     uint32_t* hist = L.hist.as<uint32_t>();
     uint32_t* totals = hist + 256 * (size_t)nb;
     uint32_t* kin = L.keys.as<uint32_t>();
@@ -516,12 +513,12 @@ cudaError_t lbvh_hierarchy(Lbvh& L, int64_t n, const uint32_t* sorted_keys, cons
                            cudaStream_t st) {
     cudaError_t e;
     int64_t ni = n > 1 ? n - 1 : 1;
-    if ((e = L.left.ensure(sizeof(int32_t) * ni)) != cudaSuccess) return e;
-    if ((e = L.right.ensure(sizeof(int32_t) * ni)) != cudaSuccess) return e;
-    if ((e = L.parent.ensure(sizeof(int32_t) * (2 * n))) != cudaSuccess) return e;
-    if ((e = L.flags.ensure(sizeof(uint32_t) * ni)) != cudaSuccess) return e;
-    if ((e = L.node_boxes.ensure(sizeof(float4) * 2 * ni)) != cudaSuccess) return e;
-    if ((e = L.nodes.ensure(sizeof(BvhNode) * ni)) != cudaSuccess) return e;
+    if ((e = L.left.ensure(LbvhBytes::child(n))) != cudaSuccess) return e;
+    if ((e = L.right.ensure(LbvhBytes::child(n))) != cudaSuccess) return e;
+    if ((e = L.parent.ensure(LbvhBytes::parent(n))) != cudaSuccess) return e;
+    if ((e = L.flags.ensure(LbvhBytes::child(n))) != cudaSuccess) return e;
+    if ((e = L.node_boxes.ensure(LbvhBytes::node_boxes(n))) != cudaSuccess) return e;
+    if ((e = L.nodes.ensure(LbvhBytes::nodes(n))) != cudaSuccess) return e;
     L.n = n;
     if (n > 1) {
         k_karras<<<blocks_for(n - 1, 256), 256, 0, st>>>(sorted_keys, n, L.left.as<int32_t>(),
@@ -539,8 +536,8 @@ cudaError_t lbvh_hierarchy(Lbvh& L, int64_t n, const uint32_t* sorted_keys, cons
 
 cudaError_t morton_sort_boxes(Lbvh& L, int64_t n, const float4* boxes, cudaStream_t st) {
     cudaError_t e;
-    if ((e = L.keys.ensure(sizeof(uint32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.bounds.ensure(sizeof(uint32_t) * 8)) != cudaSuccess) return e;
+    if ((e = L.keys.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.bounds.ensure(LbvhBytes::bounds())) != cudaSuccess) return e;
     k_bounds_init<<<1, 32, 0, st>>>(L.bounds.as<uint32_t>()); gvc::note_launch();
     unsigned nbk = blocks_for(n, 256);
     if (nbk > 148u * 8u) nbk = 148u * 8u;
@@ -552,8 +549,8 @@ cudaError_t morton_sort_boxes(Lbvh& L, int64_t n, const float4* boxes, cudaStrea
 
 cudaError_t morton_sort_points(Lbvh& L, int64_t n, const float* pts, cudaStream_t st) {
     cudaError_t e;
-    if ((e = L.keys.ensure(sizeof(uint32_t) * n)) != cudaSuccess) return e;
-    if ((e = L.bounds.ensure(sizeof(uint32_t) * 8)) != cudaSuccess) return e;
+    if ((e = L.keys.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.bounds.ensure(LbvhBytes::bounds())) != cudaSuccess) return e;
     k_bounds_init<<<1, 32, 0, st>>>(L.bounds.as<uint32_t>()); gvc::note_launch();
     unsigned nbk = blocks_for(n, 256);
     if (nbk > 148u * 8u) nbk = 148u * 8u;
@@ -570,7 +567,7 @@ cudaError_t lbvh_build_boxes(Lbvh& L, int64_t n, const float4* boxes, cudaStream
         return cudaSuccess;
     }
     if ((e = morton_sort_boxes(L, n, boxes, st)) != cudaSuccess) return e;
-    if ((e = L.sorted_boxes.ensure(sizeof(float4) * 2 * n)) != cudaSuccess) return e;
+    if ((e = L.sorted_boxes.ensure(LbvhBytes::sorted_boxes(n))) != cudaSuccess) return e;
     k_gather_boxes<<<blocks_for(n, 256), 256, 0, st>>>(n, L.perm.as<int32_t>(), boxes, L.sorted_boxes.as<float4>()); gvc::note_launch();
     return lbvh_hierarchy(L, n, L.keys.as<uint32_t>(), L.sorted_boxes.as<float4>(), st);
 }

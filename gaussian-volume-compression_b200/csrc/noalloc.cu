@@ -11,8 +11,16 @@
 //
 // Set-up: the first call on a device, with that device current, looks up the array's
 // device address with cudaGetSymbolAddress (the array's name is only a host-side
-// stand-in in host code) and caches it for that device.  That first call should come
-// before any stream capture on the device.
+// stand-in in host code) and caches it for that device.  Under CUDA's default lazy
+// module loading that lookup is also when the driver loads this library's device code
+// on the device and reserves the array, so the first call per device does reserve
+// device memory once; a call with N = 0 does only this set-up, and callers that must not
+// allocate later make it at start-up (or run with CUDA_MODULE_LOADING=EAGER, which
+// reserves the array when the library's device code loads).  That first call should
+// come before any stream capture on the device.
+//
+// Every call returns after `stream` has finished the call's work: it reads the traversal
+// status word back to the host.
 //
 // Every call shares the array and it keeps the last call's contents; whatever must
 // start at zero is cleared on each call.  Calls whose work overlaps on the GPU (two
@@ -31,25 +39,28 @@ constexpr size_t kAlign = 256;
 
 constexpr size_t up(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
 
-// Regions carved out of the array for kStaticMaxCells cells.
+// Regions carved out of the array for kStaticMaxCells cells, each sized by the LBVH
+// builder's own rules (LbvhBytes) for that many boxes.
 constexpr int64_t kC = kStaticMaxCells;
-constexpr int64_t kHistBlocks = (kC + 4095) / 4096;
+using gvc::LbvhBytes;
 constexpr size_t kOffStatus = 0;
 constexpr size_t kOffBoxes = kOffStatus + up(sizeof(int));
 constexpr size_t kOffKeys = kOffBoxes + up(32 * kC);
-constexpr size_t kOffKeysAlt = kOffKeys + up(4 * kC);
-constexpr size_t kOffPerm = kOffKeysAlt + up(4 * kC);
-constexpr size_t kOffPermAlt = kOffPerm + up(4 * kC);
-constexpr size_t kOffHist = kOffPermAlt + up(4 * kC);
-constexpr size_t kOffBounds = kOffHist + up(4 * (256 * kHistBlocks + 256));
-constexpr size_t kOffSorted = kOffBounds + up(32);
-constexpr size_t kOffLeft = kOffSorted + up(32 * kC);
-constexpr size_t kOffRight = kOffLeft + up(4 * kC);
-constexpr size_t kOffParent = kOffRight + up(4 * kC);
-constexpr size_t kOffFlags = kOffParent + up(8 * kC);
-constexpr size_t kOffNodeBoxes = kOffFlags + up(4 * kC);
-constexpr size_t kOffNodes = kOffNodeBoxes + up(32 * kC);
-constexpr size_t kScratchBytes = kOffNodes + up(64 * kC);  // about 6.4 MB
+constexpr size_t kOffKeysAlt = kOffKeys + up(LbvhBytes::keys(kC));
+constexpr size_t kOffPerm = kOffKeysAlt + up(LbvhBytes::keys(kC));
+constexpr size_t kOffPermAlt = kOffPerm + up(LbvhBytes::keys(kC));
+constexpr size_t kOffHist = kOffPermAlt + up(LbvhBytes::keys(kC));
+constexpr size_t kOffBounds = kOffHist + up(LbvhBytes::hist(kC));
+constexpr size_t kOffSorted = kOffBounds + up(LbvhBytes::bounds());
+constexpr size_t kOffLeft = kOffSorted + up(LbvhBytes::sorted_boxes(kC));
+constexpr size_t kOffRight = kOffLeft + up(LbvhBytes::child(kC));
+constexpr size_t kOffParent = kOffRight + up(LbvhBytes::child(kC));
+constexpr size_t kOffFlags = kOffParent + up(LbvhBytes::parent(kC));
+constexpr size_t kOffNodeBoxes = kOffFlags + up(LbvhBytes::child(kC));
+constexpr size_t kOffNodes = kOffNodeBoxes + up(LbvhBytes::node_boxes(kC));
+constexpr size_t kScratchBytes = kOffNodes + up(LbvhBytes::nodes(kC));  // about 6.4 MB
+static_assert(kScratchBytes < (size_t(8) << 20), "the static scratch array is meant to stay modest");
+static_assert(kOffBoxes % 16 == 0 && kOffSorted % 16 == 0 && kOffNodes % 64 == 0, "region alignment");
 
 }  // namespace
 
@@ -104,8 +115,6 @@ extern "C" int gvc_sample_tets_static(int64_t npts, const float* pts, int64_t C,
         set_msg(errbuf, errbuf_len, "gvc_sample_tets_static: null mesh pointer");
         return GVC_ERR_ARG;
     }
-    if (N == 0) return GVC_OK;
-
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -126,6 +135,7 @@ extern "C" int gvc_sample_tets_static(int64_t npts, const float* pts, int64_t C,
         }
         base = static_cast<unsigned char*>(g_scratch_addr[dev]);
     }
+    if (N == 0) return GVC_OK;  // set-up only
     cudaStream_t st = (cudaStream_t)stream;
     int* d_status = reinterpret_cast<int*>(base + kOffStatus);
     if ((e = cudaMemsetAsync(d_status, 0, sizeof(int), st)) != cudaSuccess) {
@@ -136,19 +146,38 @@ extern "C" int gvc_sample_tets_static(int64_t npts, const float* pts, int64_t C,
     const int32_t* cperm = nullptr;
     if (C > 0) {
         gvc::Lbvh L;  // views of the static array: every ensure() below fits, nothing is allocated
-        L.keys = view(base, kOffKeys, 4 * kC);
-        L.keys_alt = view(base, kOffKeysAlt, 4 * kC);
-        L.perm = view(base, kOffPerm, 4 * kC);
-        L.perm_alt = view(base, kOffPermAlt, 4 * kC);
-        L.hist = view(base, kOffHist, 4 * (256 * kHistBlocks + 256));
-        L.bounds = view(base, kOffBounds, 32);
-        L.sorted_boxes = view(base, kOffSorted, 32 * kC);
-        L.left = view(base, kOffLeft, 4 * kC);
-        L.right = view(base, kOffRight, 4 * kC);
-        L.parent = view(base, kOffParent, 8 * kC);
-        L.flags = view(base, kOffFlags, 4 * kC);
-        L.node_boxes = view(base, kOffNodeBoxes, 32 * kC);
-        L.nodes = view(base, kOffNodes, 64 * kC);
+        L.keys = view(base, kOffKeys, LbvhBytes::keys(kC));
+        L.keys_alt = view(base, kOffKeysAlt, LbvhBytes::keys(kC));
+        L.perm = view(base, kOffPerm, LbvhBytes::keys(kC));
+        L.perm_alt = view(base, kOffPermAlt, LbvhBytes::keys(kC));
+        L.hist = view(base, kOffHist, LbvhBytes::hist(kC));
+        L.bounds = view(base, kOffBounds, LbvhBytes::bounds());
+        L.sorted_boxes = view(base, kOffSorted, LbvhBytes::sorted_boxes(kC));
+        L.left = view(base, kOffLeft, LbvhBytes::child(kC));
+        L.right = view(base, kOffRight, LbvhBytes::child(kC));
+        L.parent = view(base, kOffParent, LbvhBytes::parent(kC));
+        L.flags = view(base, kOffFlags, LbvhBytes::child(kC));
+        L.node_boxes = view(base, kOffNodeBoxes, LbvhBytes::node_boxes(kC));
+        L.nodes = view(base, kOffNodes, LbvhBytes::nodes(kC));
+        // every view must hold what the builder asks for C boxes; then none of its
+        // ensure() calls reallocates (an undersized view would be freed as if it were
+        // allocated memory)
+        const struct {
+            const gvc::DevBuf& b;
+            size_t need;
+        } need[] = {{L.keys, LbvhBytes::keys(C)},          {L.keys_alt, LbvhBytes::keys(C)},
+                    {L.perm, LbvhBytes::keys(C)},          {L.perm_alt, LbvhBytes::keys(C)},
+                    {L.hist, LbvhBytes::hist(C)},          {L.bounds, LbvhBytes::bounds()},
+                    {L.sorted_boxes, LbvhBytes::sorted_boxes(C)}, {L.left, LbvhBytes::child(C)},
+                    {L.right, LbvhBytes::child(C)},        {L.parent, LbvhBytes::parent(C)},
+                    {L.flags, LbvhBytes::child(C)},        {L.node_boxes, LbvhBytes::node_boxes(C)},
+                    {L.nodes, LbvhBytes::nodes(C)}};
+        for (const auto& r : need) {
+            if (r.b.bytes < r.need) {
+                set_msg(errbuf, errbuf_len, "gvc_sample_tets_static: scratch layout too small");
+                return GVC_ERR_CAPACITY;
+            }
+        }
         const void* before[] = {L.keys.ptr, L.keys_alt.ptr, L.perm.ptr, L.perm_alt.ptr, L.hist.ptr, L.bounds.ptr,
                                 L.sorted_boxes.ptr, L.left.ptr, L.right.ptr, L.parent.ptr, L.flags.ptr,
                                 L.node_boxes.ptr, L.nodes.ptr};

@@ -185,10 +185,14 @@ int gvc_training_samples(gvc_ctx* ctx, int64_t npts, const float* pts, int64_t C
    static device array of about 6.4 MB in every device that loads the library, which
    limits the mesh to C <= 32768 cells (larger meshes are rejected with
    GVC_ERR_CAPACITY and a message in errbuf).  The first call on a device looks up the
-   array's device address and should come before any stream capture on that device.
-   Calls share the array: calls that overlap on the GPU race, so issue them one after
-   another.  Samples are traversed in the caller's order; the call waits for `stream`
-   to report a traversal overflow.  errbuf (host, may be NULL) receives a message. */
+   array's device address; under CUDA's default lazy module loading that is also when
+   the driver loads the library's device code there and reserves the array, so that
+   first call reserves device memory once.  A call with N = 0 does only this set-up:
+   make it at start-up (or run with CUDA_MODULE_LOADING=EAGER), and before any stream
+   capture on that device.  Later calls allocate nothing.  Calls share the array: calls
+   that overlap on the GPU race, so issue them one after another.  Samples are traversed
+   in the caller's order; the call returns after `stream` has finished its work (it
+   reads the traversal status back).  errbuf (host, may be NULL) receives a message. */
 int gvc_sample_tets_static(int64_t npts, const float* pts, int64_t C, const int32_t* conn4, const double* values,
                            int64_t N, const float* samples, double* out, int64_t* cell_ids, void* stream,
                            char* errbuf, int64_t errbuf_len);

@@ -1,0 +1,3 @@
+// cuda_runtime.h -- empty host stand-in (TEST INFRASTRUCTURE ONLY): the prelude supplies the CUDA
+// types and qualifiers the reference rasterizer uses.
+#pragma once

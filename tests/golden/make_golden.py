@@ -2,6 +2,8 @@
 
     python tests/golden/make_golden.py [reference_root]
 
+The reference root is the argument, else $GVC_REFERENCE_ROOT.
+
 The reference modules import packages that are absent here (plyfile, pyvista,
 simple_knn, the CUDA extensions), so the functions on the hot path's Python side are
 extracted from the reference sources with `ast` and executed as written:
@@ -25,7 +27,9 @@ import textwrap
 import numpy as np
 import torch
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GVC_REFERENCE_ROOT", "")
+if not os.path.isdir(REF):
+    sys.exit("usage: make_golden.py REFERENCE_ROOT (or set GVC_REFERENCE_ROOT)")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_python.npz")
 
 
