@@ -17,10 +17,11 @@ the reference's training loop does per iteration on this path: build the sample 
 N > 1 (torchrun): weak scaling -- every rank holds all Gaussians and its own 16M
 samples; the per-Gaussian gradients are summed with one NCCL all-reduce per step.
 
---impl reference: the reference's evaluation formula restated on the CPU (the oracle:
-the reference's CUDA extension cannot be built -- its cuBQL/glm/Viskores sources are not
-vendored), timed on bounded samples with all host threads and extrapolated to the full
-step; rank 0 only.
+--impl reference: the reference's own rasterizer kernels (forward.cu, backward.cu)
+compiled for the host CPU (oracle/_ref; the reference's CUDA extension cannot be built on
+the GPU -- its cuBQL/glm sources are not vendored), in its default sample-BVH mode, timed
+on bounded samples of the points with all host threads and extrapolated to the full step;
+rank 0 only.  Without oracle/_ref it falls back to the FP64 restatement (oracle/).
 """
 import argparse
 import json
@@ -163,56 +164,104 @@ def measured_peaks():
 
 
 # ----------------------------------------------------------------------------------------
-# CPU baseline: the oracle (the reference formula restated in C, OpenMP) on bounded samples
+# CPU legs: the reference's own rasterizer kernels compiled for the host (oracle/_ref,
+# "reference"), else the FP64 restatement (oracle/gvc_oracle.c, "port"), on bounded
+# samples of the workload's points with all Gaussians, extrapolated linearly in S
 # ----------------------------------------------------------------------------------------
-def cpu_step_time(means, scales, rots, values, weights, samples, n_sub, seed=5):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
+def _oracle_path():
+    p = os.path.join(ROOT, "oracle")
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def cpu_kind():
+    _oracle_path()
+    import refslice
+    return "reference" if refslice.available() else "port"
+
+
+def cpu_step_time(kind, means, scales, rots, values, weights, samples, n_sub, seed=5):
+    """One CPU step on n_sub of the points: preprocess, forward, masked-L1 gradient,
+    backward (covariance adjoint included).  kind "reference": the reference's kernels in
+    its default (sample-BVH) mode, FP32, all host threads; "port": the FP64 oracle."""
+    _oracle_path()
     rng = np.random.default_rng(seed)
     sub = samples[rng.choice(samples.shape[0], n_sub, replace=False)]
+    gt = (0.5 + 0.4 * np.sin(6 * sub[:, 0]) * np.sin(5 * sub[:, 1]) * np.sin(4 * sub[:, 2])).astype(np.float32)
     t0 = time.perf_counter()
-    c32, _, bb = oracle.preprocess(means, scales, rots, weights)
-    out, outw = oracle.forward(means, values, weights, c32.astype(np.float64), bb, sub)
-    gt = 0.5 + 0.4 * np.sin(6 * sub[:, 0]) * np.sin(5 * sub[:, 1]) * np.sin(4 * sub[:, 2])
-    mask = out != -1
-    g = np.where(mask, np.sign(out - gt), 0.0) / max(int(mask.sum()), 1)
-    r = oracle.backward(means, values, weights, c32.astype(np.float64), bb, sub, out.astype(np.float32),
-                        outw.astype(np.float32), g.astype(np.float32), np.zeros(n_sub, np.float32))
-    oracle.cov_backward(scales, rots, c32, r["dconics"])
+    if kind == "reference":
+        import refslice
+        rc, rb = refslice.preprocess(means, scales, rots, weights)
+        out, outw, _ = refslice.forward(means, values, weights, sub, rc, rb, use_gaussian_bvh=False)
+        mask = out != -1
+        g = (np.where(mask, np.sign(out - gt), 0.0) / max(int(mask.sum()), 1)).astype(np.float32)
+        refslice.backward(means, scales, rots, rc, values, weights, rb, sub, out, outw, g,
+                          np.zeros(n_sub, np.float32), use_gaussian_bvh=False)
+    else:
+        import oracle
+        c32, _, bb = oracle.preprocess(means, scales, rots, weights)
+        out, outw = oracle.forward(means, values, weights, c32.astype(np.float64), bb, sub)
+        mask = out != -1
+        g = np.where(mask, np.sign(out - gt), 0.0) / max(int(mask.sum()), 1)
+        r = oracle.backward(means, values, weights, c32.astype(np.float64), bb, sub, out.astype(np.float32),
+                            outw.astype(np.float32), g.astype(np.float32), np.zeros(n_sub, np.float32))
+        oracle.cov_backward(scales, rots, c32, r["dconics"])
     return time.perf_counter() - t0
 
 
-def cpu_baseline(means, scales, rots, values, weights, samples, sizes=(250_000, 1_000_000)):
-    """Times the oracle at two sample counts and extrapolates linearly to the full S."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    oracle.lib()
+CPU_DESC = {"reference": "the reference's own kernels (diff-gaussian-rasterization/cuda_rasterizer/forward.cu, "
+                         "backward.cu) compiled for the host by oracle/build_ref.py, FP32, its default sample-BVH "
+                         "mode (forward.cu:116-182, backward.cu:127-337), OpenMP over blocks; a uniform grid stands "
+                         "in for the unvendored cuBQL BVH",
+            "port": "the oracle's FP64 restatement (oracle/gvc_oracle.c, OpenMP)"}
+
+
+def cpu_extrapolated(kind, means, scales, rots, values, weights, samples, n_a, n_b, reps_b=1, warmup=0):
+    """Times n_a points once and n_b points reps_b times (median) after `warmup` untimed
+    n_b runs; extrapolates t = fixed + slope * S to the full step."""
     threads = os.cpu_count() or 1
     S = samples.shape[0]
-    if S <= sizes[1]:
-        t = cpu_step_time(means, scales, rots, values, weights, samples, S)
-        return {"value": t * 1e3, "unit": "ms/step", "cores": threads, "kind": "port",
-                "sample": "oracle fwd+bwd (C, OpenMP %d threads) on the full step: all %d points and %d Gaussians"
-                          % (threads, S, means.shape[0]), "extrapolated": False}
-    t = [cpu_step_time(means, scales, rots, values, weights, samples, n) for n in sizes]
-    slope = (t[1] - t[0]) / (sizes[1] - sizes[0])
-    fixed = max(t[0] - slope * sizes[0], 0.0)
-    full = fixed + slope * samples.shape[0]
-    return {"value": full * 1e3, "unit": "ms/step", "cores": threads, "kind": "port",
-            "sample": "oracle fwd+bwd (C, OpenMP %d threads) on %d and %d of the %d points with all %d Gaussians "
-                      "(%.2f s, %.2f s), linearly extrapolated to the full step" %
-                      (threads, sizes[0], sizes[1], samples.shape[0], means.shape[0], t[0], t[1]),
-            "extrapolated": True}
+    t_a = cpu_step_time(kind, means, scales, rots, values, weights, samples, n_a)
+    for _ in range(warmup):
+        cpu_step_time(kind, means, scales, rots, values, weights, samples, n_b)
+    tb = [cpu_step_time(kind, means, scales, rots, values, weights, samples, n_b, seed=10 + k) for k in range(reps_b)]
+    t_b = float(np.median(tb))
+    slope = (t_b - t_a) / (n_b - n_a)
+    fixed = max(t_a - slope * n_a, 0.0)
+    full_ms = (fixed + slope * S) * 1e3
+    return {"value": full_ms, "unit": "ms/step", "cores": threads, "kind": kind,
+            "sample": "%s: fwd+bwd on %d (x1) and %d (x%d, median) of the %d points with all %d Gaussians "
+                      "(%.2f s, %.2f s per sample step), linearly extrapolated to the full step"
+                      % (CPU_DESC[kind], n_a, n_b, reps_b, S, means.shape[0], t_a, t_b),
+            "extrapolated": True,
+            "timed": {"points_a": int(n_a), "reps_a": 1, "seconds_a": t_a, "points_b": int(n_b),
+                      "reps_b": int(reps_b), "seconds_b_median": t_b, "fixed_s": fixed, "per_point_us": slope * 1e6,
+                      "full_step_equivalents": (n_a + reps_b * n_b) / S}}
 
 
-def fp64_errors(means, scales, rots, values, weights, samples, paths, n_sub=50_000, seed=7):
+def cpu_baseline(means, scales, rots, values, weights, samples):
+    """Our line's cpu_baseline: the same measurement as the reference arm, one repetition."""
+    kind = cpu_kind()
+    S = samples.shape[0]
+    if S <= 300_000:
+        threads = os.cpu_count() or 1
+        t = cpu_step_time(kind, means, scales, rots, values, weights, samples, S)
+        return {"value": t * 1e3, "unit": "ms/step", "cores": threads, "kind": kind,
+                "sample": "%s: the full step, all %d points and %d Gaussians" % (CPU_DESC[kind], S, means.shape[0]),
+                "extrapolated": False}
+    return cpu_extrapolated(kind, means, scales, rots, values, weights, samples, min(125_000, S // 8),
+                            min(500_000, S // 2))
+
+
+def fp64_errors(means, scales, rots, values, weights, samples, paths, n_sub=1_000_000, seed=7):
     """Checker, outside every timed region: each path's forward (cells = V/W and W) against
     the oracle's FP64 evaluation of the same conics at a random subset of points.  Reports
     the largest and the 99.99th-percentile relative error over points the reference marks
     valid, and the share of points above 1e-4.  Points whose W lies within 1e-6 of the 0.01
     validity threshold are left out (either answer is within rounding)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    _oracle_path()
     import oracle
+    n_sub = min(n_sub, samples.shape[0])
     rng = np.random.default_rng(seed)
     idx = np.sort(rng.choice(samples.shape[0], n_sub, replace=False))
     sub = samples[idx]
@@ -233,34 +282,91 @@ def fp64_errors(means, scales, rots, values, weights, samples, paths, n_sub=50_0
     return res
 
 
+GRAD_FIELDS = ("means", "scales", "rotations", "values", "weights")
+
+
+def grad_errors(means, scales, rots, values, weights, samples, runs, n_gauss=10_000, seed=8):
+    """Checker, outside every timed region: each backward's gradients of a random subset of
+    n_gauss Gaussians against the oracle's FP64 adjoint (backward.cu:252-298 restated) over
+    ALL samples of the step, with the same forward outputs and loss gradient the GPU used,
+    then the covariance adjoint (true gradient).  Per field: max |gpu - fp64| / max |fp64|
+    over the subset, and the 99.9th percentile of the per-Gaussian relative error."""
+    _oracle_path()
+    import oracle
+    P = means.shape[0]
+    rng = np.random.default_rng(seed)
+    sel = np.sort(rng.choice(P, min(n_gauss, P), replace=False))
+    res = {"gaussians": int(sel.size), "reference": "oracle FP64 adjoint over all samples of the step "
+                                                     "(the path's own forward outputs and conics)"}
+    for name, r in runs.items():
+        conics = r["conics"][sel]
+        _, _, bb = oracle.preprocess(means[sel], scales[sel], rots[sel], weights[sel])
+        g = oracle.backward(means[sel], values[sel], weights[sel], conics.astype(np.float64), bb, samples,
+                            r["out"], r["outw"], r["gout"], np.zeros(samples.shape[0], np.float32))
+        ds, dq = oracle.cov_backward(scales[sel], rots[sel], conics, g["dconics"])
+        ref = [g["dmeans"], ds, dq, g["dvalues"].reshape(-1, 1), g["dweights"].reshape(-1, 1)]
+        out = {}
+        for k, f in enumerate(GRAD_FIELDS):
+            got = r["grads"][k].reshape(P, -1)[sel].astype(np.float64)
+            rf = ref[k].reshape(sel.size, -1)
+            scale = np.abs(rf).max()
+            rel = np.abs(got - rf).max(1) / np.maximum(np.abs(rf).max(1), 1e-30)
+            big = np.abs(rf).max(1) > 1e-3 * scale
+            out[f] = {"max_abs_err_over_max": float(np.abs(got - rf).max() / scale) if scale > 0 else 0.0,
+                      "p999_rel_err": float(np.quantile(rel[big], 0.999)) if big.any() else 0.0}
+        res[name] = out
+    return res
+
+
+def config_dict(args, desc, P, S, world):
+    """The config object of both arms' lines (identical for the same arguments)."""
+    return {"workload": desc, "P": P, "S_per_gpu": S, "path": args.eval_path, "backward": args.bwd_mode,
+            "use_gaussian_bvh": bool(args.use_gaussian_bvh),
+            "l2": "inputs larger than L2 (samples %d MB, Gaussian records %d MB)" % (S * 12 // 2**20, P * 80 // 2**20),
+            "parallelism": "samples sharded per rank, NCCL all-reduce of gradients" if world > 1 else "single GPU"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     means, scales, rots, values, weights, samples, desc = workload(args.config, 0)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    oracle.lib()
-    threads = os.cpu_count() or 1
+    kind = cpu_kind()
     S = samples.shape[0]
-    n_a, n_b = min(125_000, S // 4), min(500_000, S)
-    t_a = cpu_step_time(means, scales, rots, values, weights, samples, n_a)
-    for _ in range(max(args.warmup - 1, 0)):
-        cpu_step_time(means, scales, rots, values, weights, samples, n_b)
-    times = [cpu_step_time(means, scales, rots, values, weights, samples, n_b, seed=10 + k) for k in range(args.steps)]
-    t_b = float(np.median(times))
-    slope = (t_b - t_a) / (n_b - n_a)
-    full_ms = (max(t_a - slope * n_a, 0.0) + slope * S) * 1e3
+    if S <= 300_000:
+        for _ in range(args.warmup):
+            cpu_step_time(kind, means, scales, rots, values, weights, samples, S)
+        t = [cpu_step_time(kind, means, scales, rots, values, weights, samples, S, seed=10 + k)
+             for k in range(args.steps)]
+        full_ms = float(np.median(t)) * 1e3
+        cpu = {"value": full_ms, "unit": "ms/step", "cores": os.cpu_count() or 1, "kind": kind,
+               "sample": "%s: the full step (all %d points, %d Gaussians), median of %d" %
+                         (CPU_DESC[kind], S, means.shape[0], args.steps), "extrapolated": False}
+        extra = {"extrapolated": False}
+    else:
+        # each sample step: all Gaussians and n_b of the points, sized so that the whole
+        # run stays within a few minutes on the host cores
+        n_a, n_b = min(62_500, S // 16), min(250_000, S // 4)
+        cpu = cpu_extrapolated(kind, means, scales, rots, values, weights, samples, n_a, n_b, reps_b=args.steps,
+                               warmup=max(args.warmup - 1, 0))
+        full_ms = cpu["value"]
+        extra = {"extrapolated": True,
+                 "steps_note": "each of the %d steps is a bounded sample (%d of the %d points, all Gaussians); "
+                               "value and ms_per_step are the linear extrapolation to the full step, and the "
+                               "timed work equals %.3f full steps" % (args.steps, n_b, S,
+                                                                       cpu["timed"]["full_step_equivalents"])}
     line = {"metric": METRIC, "value": full_ms, "unit": "ms/step", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_ms, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "P": means.shape[0], "S": S},
-            "cpu_baseline": {"value": full_ms, "unit": "ms/step", "cores": threads, "kind": "port",
-                             "sample": "oracle fwd+bwd on %d (x1) and %d (x%d, median) of %d points, all Gaussians, "
-                                       "extrapolated linearly" % (n_a, n_b, args.steps, S)},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if kind == "reference" else "f64",
+            "data": "synthetic", "config": config_dict(args, desc, means.shape[0], S, 1),
+            "cpu_baseline": cpu,
             "e2e": {"value": full_ms, "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference CUDA extension is not buildable (cuBQL, glm and Viskores sources absent); "
-                    "this arm is the reference formula restated in C (oracle/gvc_oracle.c)"}
+            "note": "the reference's CUDA extension cannot be built on the GPU (its cuBQL and glm sources are not "
+                    "vendored); this arm runs the reference's own kernel source compiled for the host CPU"
+                    if kind == "reference" else
+                    "the reference's sources were not available where oracle/_ref is built; this arm is the "
+                    "oracle's FP64 restatement"}
+    line.update(extra)
     print(json.dumps(line), flush=True)
 
 
@@ -311,11 +417,17 @@ def mesh_bench(dev, steps, warmup, with_cpu):
         import oracle
         sub = q[:1_000_000]
         t0 = time.perf_counter()
-        oracle.sample_tets(pts, tets, vals, sub)
+        r_out, r_cell = oracle.sample_tets(pts, tets, vals, sub)
         t = time.perf_counter() - t0
         tet["cpu_oracle"] = {"points_per_s": sub.shape[0] / t, "cores": os.cpu_count() or 1,
                              "sample": "oracle (C, OpenMP, uniform grid locator) on 1M of the points, "
                                        "locator build included (%.2f s)" % t}
+        g_out = d_out[:sub.shape[0]].cpu().numpy()
+        g_cell = d_cell[:sub.shape[0]].cpu().numpy()
+        tet["bit_exact_vs_oracle"] = {"points": int(sub.shape[0]),
+                                      "cell_ids": bool(np.array_equal(g_cell, r_cell)),
+                                      "values": bool(np.array_equal(g_out, r_out)),
+                                      "cell_id_mismatches": int((g_cell != r_cell).sum())}
     res["tets"] = tet
     # training batches (train.py:34-61, :273-315): 100 batches of 128^3 points in random
     # tetrahedra, per-batch Morton sort, float32 ground truth, all on the device
@@ -576,9 +688,10 @@ def run_ours(args):
                        "(samples, their target values, parameters; double-buffered on a copy stream) and "
                        "reads its loss back to pinned host memory (checked on the host while the next step runs)"}
 
-    # the two evaluation paths side by side: full step time and forward outputs (kept on the
-    # host for the FP64 comparison below)
+    # the two evaluation paths side by side: full step time, forward outputs and the
+    # gradients of one step (kept on the host for the FP64 comparisons below)
     paths = {}
+    grad_runs = {}
     paths_extra = {}
     if not args.profile:
         # (forward path, backward mode): FP32 throughout, tensor cores throughout, and the FP32
@@ -599,14 +712,23 @@ def run_ours(args):
             b1.record(stream)
             torch.cuda.synchronize()
             pm = gvc_dist.max_over_ranks(b0.elapsed_time(b1) / args.steps, dev)
-            if name == "plain_fwd_tc_bwd":
-                paths_extra = {"plain_fwd_tc_bwd_ms_per_step": pm}
-                continue
+            # one more step, outputs and gradients kept (untimed)
             _C.build_bvh(d_samples, False, ugb)
             o, ow, cn = _C.rasterize_gaussians(d_means, d_scales, d_rots, d_values, d_weights, 1.0, *bounds, -1.0,
                                                ugb, False)
-            paths[name] = {"ms_per_step": pm, "out": o.cpu().numpy(), "outw": ow.cpu().numpy(),
-                           "conics": cn.cpu().numpy().reshape(-1, 6)}
+            mask = (o != -1) & (d_gt != -1)
+            gl = torch.where(mask, torch.sign(o - d_gt), torch.zeros_like(o)) / mask.sum().clamp_min(1)
+            gr = _C.rasterize_gaussians_backward(d_means, d_scales, d_rots, cn, d_values, d_weights, o, ow, 1.0,
+                                                 *bounds, -1.0, gl, zeros_w, ugb, False)
+            _C.check_status()
+            run = {"ms_per_step": pm, "out": o.cpu().numpy(), "outw": ow.cpu().numpy(),
+                   "conics": cn.cpu().numpy().reshape(-1, 6), "gout": gl.cpu().numpy(),
+                   "grads": [x.cpu().numpy() for x in gr]}
+            grad_runs[name] = run
+            if name == "plain_fwd_tc_bwd":
+                paths_extra = {"plain_fwd_tc_bwd_ms_per_step": pm}
+                continue
+            paths[name] = run
         _C.set_eval_path(args.eval_path)
         _C.set_backward_mode(args.bwd_mode)
         _C.check_status()
@@ -616,11 +738,15 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
         cpu = cpu_baseline(means, scales, rots, values, weights, samples)
         fp64 = fp64_errors(means, scales, rots, values, weights, samples, paths)
+        fp64["gradients"] = grad_errors(means, scales, rots, values, weights, samples, grad_runs)
     tc_vs_plain = None
     if paths:
         tc_vs_plain = {"plain_ms_per_step": paths["plain"]["ms_per_step"],
                        "tensor_core_ms_per_step": paths["tensor_core"]["ms_per_step"],
                        "speedup_tc_over_plain": paths["plain"]["ms_per_step"] / paths["tensor_core"]["ms_per_step"],
+                       "paths": {"plain": "FP32 CTA forward + FP32 deterministic Gaussian-owned backward",
+                                 "tensor_core": "tcgen05 split-BF16 exponent forward + tcgen05 moment backward",
+                                 "plain_fwd_tc_bwd": "FP32 CTA forward + tcgen05 moment backward"},
                        "fp64_error": fp64}
         tc_vs_plain.update(paths_extra)
 
@@ -628,12 +754,7 @@ def run_ours(args):
         line = {"metric": METRIC, "value": ms, "unit": "ms/step", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": desc, "P": P, "S_per_gpu": S, "path": args.eval_path,
-                           "backward": args.bwd_mode, "use_gaussian_bvh": ugb,
-                           "l2": "inputs larger than L2 (samples %d MB, Gaussian records %d MB)" %
-                                 (S * 12 // 2**20, P * 80 // 2**20),
-                           "parallelism": "samples sharded per rank, NCCL all-reduce of gradients" if world > 1
-                           else "single GPU"},
+                "config": config_dict(args, desc, P, S, world),
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e, "tc_vs_plain": tc_vs_plain,
                 "gpu_launches": int(launches), "gpu_launches_per_step": launches / args.steps}
         if args.knn and world == 1:

@@ -1,8 +1,7 @@
 // cooperative_groups.h -- host stand-in for the cooperative-groups calls of the reference
 // rasterizer (TEST INFRASTRUCTURE ONLY): grid and block handles with thread_rank(), and
-// tiled_partition<N>.  A tile of one thread is exact; wider tiles exist so that the
-// warp-per-Gaussian kernels compile, and their reductions abort if ever reached (the
-// host build launches only the thread-per-sample kernels).
+// tiled_partition<N> (a tile of N consecutive threads; its reduction is emulated in
+// cooperative_groups/reduce.h).
 #pragma once
 
 namespace cooperative_groups {

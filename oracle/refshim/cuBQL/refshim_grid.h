@@ -31,8 +31,11 @@ struct RefGrid {
                a.upper.y >= b.lower.y && a.lower.z <= b.upper.z && a.upper.z >= b.lower.z;
     }
 
-    // Primitive boxes as float[6] (lo xyz, hi xyz); `per_cell` primitives per cell on average.
-    void build(const float* b6, int64_t count, double per_cell = 2.0) {
+    // Primitive boxes as float[6] (lo xyz, hi xyz).  A cell is about half the median box
+    // extent on each axis (a box then spans about 3 x 3 x 3 cells).  Cells are filled in
+    // parallel and each cell's list is then sorted, so the index does not depend on the
+    // thread count.
+    void build(const float* b6, int64_t count) {
         boxes.resize(count);
         float L[3] = {INFINITY, INFINITY, INFINITY}, H[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (int64_t i = 0; i < count; i++) {
@@ -43,41 +46,52 @@ struct RefGrid {
                 H[a] = std::max(H[a], b6[6 * i + 3 + a]);
             }
         }
-        const int side = std::max(1, std::min(256, (int)std::cbrt((double)count / per_cell)));
         for (int a = 0; a < 3; a++) {
+            std::vector<float> e;
+            e.reserve(std::min<int64_t>(count, 100000));
+            const int64_t stride = count > 100000 ? count / 100000 : 1;
+            for (int64_t i = 0; i < count; i += stride) {
+                const float w = b6[6 * i + 3 + a] - b6[6 * i + a];
+                if (w >= 0.f) e.push_back(w);
+            }
+            float med = 0.f;
+            if (!e.empty()) {
+                std::nth_element(e.begin(), e.begin() + e.size() / 2, e.end());
+                med = e[e.size() / 2];
+            }
             lo[a] = count ? L[a] : 0.f;
             const float ext = count ? H[a] - L[a] : 0.f;
-            n[a] = ext > 0.f ? side : 1;
+            const double want = med > 0.f ? (double)ext / (0.5 * med) : std::cbrt((double)count);
+            n[a] = ext > 0.f ? (int)std::max(1.0, std::min(1024.0, want)) : 1;
             inv[a] = ext > 0.f ? (float)n[a] / ext : 0.f;
         }
         const int64_t nc = (int64_t)n[0] * n[1] * n[2];
         std::vector<int64_t> cnt(nc + 1, 0);
-        auto range = [&](const box3f& b, int (&c0)[3], int (&c1)[3]) {
-            c0[0] = cell(0, b.lower.x); c1[0] = cell(0, b.upper.x);
-            c0[1] = cell(1, b.lower.y); c1[1] = cell(1, b.upper.y);
-            c0[2] = cell(2, b.lower.z); c1[2] = cell(2, b.upper.z);
+        auto visit = [&](int64_t i, bool fill) {
+            const box3f& b = boxes[i];
+            if (!(b.lower.x <= b.upper.x && b.lower.y <= b.upper.y && b.lower.z <= b.upper.z)) return;
+            const int x0 = cell(0, b.lower.x), x1 = cell(0, b.upper.x), y0 = cell(1, b.lower.y),
+                      y1 = cell(1, b.upper.y), z0 = cell(2, b.lower.z), z1 = cell(2, b.upper.z);
+            for (int z = z0; z <= z1; z++)
+                for (int y = y0; y <= y1; y++)
+                    for (int x = x0; x <= x1; x++) {
+                        const int64_t c = ((int64_t)z * n[1] + y) * n[0] + x;
+                        int64_t slot;
+#pragma omp atomic capture
+                        slot = cnt[c]++;
+                        if (fill) ids[start[c] + slot] = (uint32_t)i;
+                    }
         };
-        for (int pass = 0; pass < 2; pass++) {
-            if (pass == 1) {
-                start.assign(nc + 1, 0);
-                for (int64_t c = 0; c < nc; c++) start[c + 1] = start[c] + cnt[c];
-                ids.resize(start[nc]);
-                std::fill(cnt.begin(), cnt.end(), 0);
-            }
-            for (int64_t i = 0; i < count; i++) {
-                const box3f& b = boxes[i];
-                if (!(b.lower.x <= b.upper.x && b.lower.y <= b.upper.y && b.lower.z <= b.upper.z)) continue;
-                int c0[3], c1[3];
-                range(b, c0, c1);
-                for (int z = c0[2]; z <= c1[2]; z++)
-                    for (int y = c0[1]; y <= c1[1]; y++)
-                        for (int x = c0[0]; x <= c1[0]; x++) {
-                            const int64_t c = ((int64_t)z * n[1] + y) * n[0] + x;
-                            if (pass == 1) ids[start[c] + cnt[c]] = (uint32_t)i;
-                            cnt[c]++;
-                        }
-            }
-        }
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < count; i++) visit(i, false);
+        start.assign(nc + 1, 0);
+        for (int64_t c = 0; c < nc; c++) start[c + 1] = start[c] + cnt[c];
+        ids.resize(start[nc]);
+        std::fill(cnt.begin(), cnt.end(), 0);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < count; i++) visit(i, true);
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int64_t c = 0; c < nc; c++) std::sort(ids.begin() + start[c], ids.begin() + start[c + 1]);
     }
 
     // Every primitive whose closed box overlaps q, ascending, each once.

@@ -8,8 +8,9 @@
 //     threadIdx/blockIdx/blockDim/gridDim (thread-local, set by ref_launch);
 //   * a kernel launch `k<<<grid, block>>>(args)` (rewritten by the recipe into
 //     ref_launch(grid, block, k, args)) runs every thread of every block in turn, blocks
-//     spread over OpenMP threads.  The emulated kernels use no shared memory, no block
-//     barriers and, for the kernels that are launched, no warp collectives;
+//     spread over OpenMP threads.  Within each warp the lanes run from 31 down to 0, so
+//     that a warp reduction (cooperative_groups/reduce.h) can hand lane 0 the sum of the
+//     lanes that ran before it; the kernels use no shared memory and no block barriers;
 //   * CUDA's float min/max (fminf/fmaxf: a NaN operand is dropped) and atomicAdd;
 //   * the float overloads of exp/abs/sqrt that CUDA device code resolves to.
 #pragma once
@@ -65,6 +66,8 @@ extern thread_local dim3 gridDim;
 // Set by the driver: when nonzero, atomicAdd is a plain add and launches run on one
 // thread in launch order (reproducible sums).
 extern int ref_serial;
+// Incremented before every emulated thread runs (resets the warp-reduction call count).
+extern thread_local unsigned long long ref_thread_epoch;
 
 inline float atomicAdd(float* p, float v) {
     float old;
@@ -91,28 +94,28 @@ inline int atomicAdd(int* p, int v) {
 }
 
 template <class K, class... A>
-void ref_launch(dim3 grid, dim3 block, K kernel, A... args) {
-    const long nb = (long)grid.x;
-    if (ref_serial) {
-        for (long b = 0; b < nb; b++) {
-            blockIdx = uint3{(unsigned)b, 0u, 0u};
-            blockDim = block;
-            gridDim = grid;
-            for (unsigned t = 0; t < block.x; t++) {
-                threadIdx = uint3{t, 0u, 0u};
-                kernel(args...);
-            }
-        }
-        return;
-    }
-#pragma omp parallel for schedule(dynamic, 4)
-    for (long b = 0; b < nb; b++) {
-        blockIdx = uint3{(unsigned)b, 0u, 0u};
-        blockDim = block;
-        gridDim = grid;
-        for (unsigned t = 0; t < block.x; t++) {
+inline void ref_run_block(long b, dim3 grid, dim3 block, K kernel, A... args) {
+    blockIdx = uint3{(unsigned)b, 0u, 0u};
+    blockDim = block;
+    gridDim = grid;
+    for (unsigned w = 0; w * 32 < block.x; w++) {
+        for (int l = 31; l >= 0; l--) {
+            const unsigned t = w * 32 + (unsigned)l;
+            if (t >= block.x) continue;
             threadIdx = uint3{t, 0u, 0u};
+            ref_thread_epoch++;
             kernel(args...);
         }
     }
+}
+
+template <class K, class... A>
+void ref_launch(dim3 grid, dim3 block, K kernel, A... args) {
+    const long nb = (long)grid.x;
+    if (ref_serial) {
+        for (long b = 0; b < nb; b++) ref_run_block(b, grid, block, kernel, args...);
+        return;
+    }
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long b = 0; b < nb; b++) ref_run_block(b, grid, block, kernel, args...);
 }

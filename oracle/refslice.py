@@ -46,9 +46,9 @@ def lib(fma=False):
         L.gvc_ref_openmp.restype = i32
         L.gvc_ref_config.argtypes = [i32, i32]
         L.gvc_ref_preprocess.argtypes = [i32, vp, vp, f32, vp, vp, vp, vp]
-        L.gvc_ref_forward.argtypes = [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.gvc_ref_forward.argtypes = [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32]
         L.gvc_ref_backward.argtypes = [i32, i32, vp, vp, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
-                                       vp, vp, vp]
+                                       vp, vp, vp, i32]
         _libs[fma] = L
     return _libs[fma]
 
@@ -76,22 +76,26 @@ def preprocess(means, scales, rots, weights, scale_modifier=1.0, fma=False):
     return conics, aabbs
 
 
-def forward(means, values, weights, samples, conics, aabbs, fma=False):
-    """Gaussian-BVH forward (forward.cu:185-259): (out [S], outw [S], counts [S])."""
+def forward(means, values, weights, samples, conics, aabbs, fma=False, use_gaussian_bvh=True):
+    """Forward: (out [S], outw [S], counts).  use_gaussian_bvh: thread per sample
+    (forward.cu:185-259; counts per sample); otherwise warp per Gaussian with atomic sums
+    into the samples (forward.cu:116-182, 261-274; counts per Gaussian)."""
     means, values, weights, samples = _f(means), _f(values).reshape(-1), _f(weights).reshape(-1), _f(samples)
     conics, aabbs = _f(conics), _f(aabbs)
     P, S = means.shape[0], samples.shape[0]
     out = np.zeros(S, np.float32)
     outw = np.zeros(S, np.float32)
-    cnt = np.zeros(S, np.int32)
+    cnt = np.zeros(S if use_gaussian_bvh else P, np.int32)
     lib(fma).gvc_ref_forward(P, S, _p(means), _p(values), _p(weights), _p(samples), _p(conics), _p(aabbs),
-                             _p(out), _p(outw), _p(cnt))
+                             _p(out), _p(outw), _p(cnt), int(bool(use_gaussian_bvh)))
     return out, outw, cnt
 
 
 def backward(means, scales, rots, conics, values, weights, aabbs, samples, out, outw, gout, gw,
-             scale_modifier=1.0, fma=False):
-    """Gaussian-BVH backward (backward.cu:339-559 then :9-125).  Returns a dict of
+             scale_modifier=1.0, fma=False, use_gaussian_bvh=True):
+    """Backward: use_gaussian_bvh: thread per sample with atomic sums into the Gaussians
+    (backward.cu:339-559); otherwise warp per Gaussian with warp reductions
+    (backward.cu:127-337); then the covariance adjoint (:9-125).  Returns a dict of
     dmeans [P,3], dvalues [P], dweights [P], dscales [P,3], drots [P,4], dconics [P,6]."""
     means, scales, rots, conics = _f(means), _f(scales), _f(rots), _f(conics)
     values, weights, aabbs, samples = _f(values).reshape(-1), _f(weights).reshape(-1), _f(aabbs), _f(samples)
@@ -103,5 +107,5 @@ def backward(means, scales, rots, conics, values, weights, aabbs, samples, out, 
     lib(fma).gvc_ref_backward(P, S, _p(means), _p(scales), scale_modifier, _p(rots), _p(conics), _p(values),
                               _p(weights), _p(aabbs), _p(samples), _p(out), _p(outw), _p(gout), _p(gw),
                               _p(r["dmeans"]), _p(r["dvalues"]), _p(r["dweights"]), _p(r["dscales"]),
-                              _p(r["drots"]), _p(r["dconics"]))
+                              _p(r["drots"]), _p(r["dconics"]), int(bool(use_gaussian_bvh)))
     return r

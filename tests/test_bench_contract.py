@@ -1,6 +1,7 @@
-"""bench.py's reference arm runs on the host cores (the oracle), so its JSON contract is
-checked here without a GPU: one line with the metric, the CPU baseline description and
-a zero-copy e2e object; ranks other than 0 print nothing and exit 0."""
+"""bench.py's reference arm runs on the host cores (the reference's kernels compiled for
+the host, or the oracle), so its JSON contract is checked here without a GPU: one line
+with the metric, the CPU baseline description, a zero-copy e2e object and the same config
+object as our arm; ranks other than 0 print nothing and exit 0."""
 import json
 import os
 import subprocess
@@ -31,6 +32,13 @@ def test_reference_arm_line():
     assert line["e2e"] == {"value": line["value"], "unit": "ms/step", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert "workload" in line["config"]
+    assert line["extrapolated"] is False and cb["extrapolated"] is False
+    # the same config object as our arm prints for the same arguments
+    sys.path.insert(0, ROOT)
+    import bench
+    ns = type("A", (), {"eval_path": "plain", "bwd_mode": "tensor_core", "use_gaussian_bvh": False})()
+    P, S, desc = bench.CONFIGS["tiny"]
+    assert line["config"] == bench.config_dict(ns, desc, P, S, 1)
 
 
 def test_reference_arm_other_ranks_are_silent():

@@ -28,7 +28,7 @@ def test_uniform_bit_exact(cuda, orc, dtype):
     assert valid.mean() > 0.5 and not valid.all()
 
 
-@pytest.mark.parametrize("n,ns", [(12, 100000), (48, 1000000)])
+@pytest.mark.parametrize("n,ns", [(12, 100000), (48, 1000000), (128, 1000000)])
 def test_tets_bit_exact(cuda, orc, n, ns):
     from gpu_mesh_sampling._gpu_mesh_sampling import sample_meshu_cells
     pts, tets = orc.jittered_tet_mesh(n=n, seed=n)

@@ -239,17 +239,41 @@ def test_deterministic_backward_is_bitwise_reproducible(cuda, small_case):
         np.testing.assert_array_equal(x, y)
 
 
-def test_gradients_match_finite_differences(cuda, orc):
-    """Full chain: pre-activation params -> activations (torch) -> GaussianRasterizer
-    (GPU forward + adjoint) -> masked L1; FD in FP64 over the frozen pair set."""
-    import bvh_diff_gaussian_rasterization as R
+def _raw_params(kind):
+    """Pre-activation parameters: 'small' (512 Gaussians on a 24^3 grid) or 'config1'
+    (4096 Gaussians, means U[0,1]^3, log-scales N(log 0.02, 0.3), random quaternions,
+    weights sigmoid(N(0,1)), values U[0,1] through the sigmoid getter, 64^3 cell centres,
+    seed 0)."""
     rng = np.random.default_rng(0)
-    P, n = 512, 24
-    xyz = rng.random((P, 3))
-    raw_s = rng.normal(np.log(0.04), 0.3, (P, 3))
-    raw_q = rng.normal(size=(P, 4))
-    raw_w = rng.normal(size=(P, 1))
-    raw_v = rng.normal(size=(P, 1))
+    if kind == "small":
+        P, n = 512, 24
+        xyz = rng.random((P, 3))
+        raw_s = rng.normal(np.log(0.04), 0.3, (P, 3))
+        raw_q = rng.normal(size=(P, 4))
+        raw_w = rng.normal(size=(P, 1))
+        raw_v = rng.normal(size=(P, 1))
+    else:
+        P, n = 4096, 64
+        xyz = rng.random((P, 3))
+        raw_s = rng.normal(np.log(0.02), 0.3, (P, 3))
+        raw_q = rng.normal(size=(P, 4))
+        raw_w = rng.normal(size=(P, 1))
+        u = rng.uniform(0.01, 0.99, (P, 1))
+        raw_v = np.log(u / (1 - u))
+    return rng, n, (xyz, raw_s, raw_q, raw_w, raw_v)
+
+
+@pytest.mark.parametrize("kind,bwd_mode", [("small", "auto"), ("small", "tensor_core"), ("config1", "auto"),
+                                           ("config1", "tensor_core")])
+def test_gradients_match_finite_differences(cuda, orc, kind, bwd_mode):
+    """Full chain: pre-activation params -> activations (torch) -> GaussianRasterizer
+    (GPU forward + adjoint, the deterministic FP32 backward or the tensor-core backward the
+    benchmark times) -> masked L1; FD in FP64 over the frozen pair set (h = 1e-4, 64
+    random parameters): |an - fd| <= 1e-3 max(|fd|, 1e-3)."""
+    import bvh_diff_gaussian_rasterization as R
+    from bvh_diff_gaussian_rasterization import _C
+    rng, n, raw = _raw_params(kind)
+    xyz, raw_s, raw_q, raw_w, raw_v = raw
     samples = orc.grid_centres(n)
     gt = orc.blob_target(samples)
     m32, s32, q32, w32, v32 = [np.asarray(a, np.float32) for a in orc.activations(xyz, raw_s, raw_q, raw_w, raw_v)]
@@ -263,11 +287,15 @@ def test_gradients_match_finite_differences(cuda, orc):
     settings = R.GaussianRasterizationSettings((0, 0, 0), (1, 1, 1), n, -1.0, 1.0, False, False)
     rast = R.GaussianRasterizer(settings)
     rast.build_bvh(T(samples, cuda))
-    leaves = [torch.tensor(a, dtype=torch.float32, device=cuda, requires_grad=True)
-              for a in (xyz, raw_s, raw_q, raw_w, raw_v)]
+    leaves = [torch.tensor(a, dtype=torch.float32, device=cuda, requires_grad=True) for a in raw]
     m, s, q, w, v = orc.activations(*leaves, xp=torch)
-    cells, weights = rast(m, s, q, v, w)
-    torch.autograd.backward(cells, torch.tensor(gsel, dtype=torch.float32, device=cuda))
+    _C.set_backward_mode(bwd_mode)
+    try:
+        cells, weights = rast(m, s, q, v, w)
+        torch.autograd.backward(cells, torch.tensor(gsel, dtype=torch.float32, device=cuda))
+        _C.check_status()
+    finally:
+        _C.set_backward_mode("auto")
     # FP64 FD over the frozen pairs
     ts = torch.tensor(samples, dtype=torch.float64)
     tmask = torch.tensor(mask)
@@ -279,7 +307,7 @@ def test_gradients_match_finite_differences(cuda, orc):
         o = V / torch.where(W > 0, W, torch.ones_like(W))
         return (torch.where(tmask, o, torch.zeros_like(o)) * tg).sum()
 
-    base = [torch.tensor(a, dtype=torch.float64) for a in (xyz, raw_s, raw_q, raw_w, raw_v)]
+    base = [torch.tensor(a, dtype=torch.float64) for a in raw]
     live = np.unique(pg[mask[ps]])
     h = 1e-4
     for _ in range(64):

@@ -128,17 +128,26 @@ def test_tensor_core_backward_matches_oracle(cuda, orc, case, gw_scale, path, mo
     assert_grads_close(got, ref)
 
 
-def test_tensor_core_backward_large_clustered(cuda, orc):
-    """Scaled large-evaluation workload: tensor-core gradients agree with the deterministic
-    FP32 reduction."""
+@pytest.mark.parametrize("path,mode", [("tensor_core", "auto"), ("plain", "tensor_core"),
+                                       ("plain", "deterministic")])
+def test_backward_large_clustered_vs_oracle(cuda, orc, path, mode):
+    """Scaled large-evaluation workload (200k clustered Gaussians, 1M samples): the
+    gradients of 20k random Gaussians against the oracle's FP64 adjoint over all samples
+    of the step (with the GPU forward's own outputs), then the covariance adjoint."""
     means, scales, rots, values, weights, samples = orc.mixture_large(seed=4, P=200_000, S=1_000_000)
     case = (means, scales, rots, values, weights, samples)
     rng = np.random.default_rng(32)
     gout = rng.normal(size=samples.shape[0]).astype(np.float32)
     gw = np.zeros(samples.shape[0], np.float32)
-    a = run_backward_path(cuda, case, gout, gw, "plain", "deterministic")[0]
-    b = run_backward_path(cuda, case, gout, gw, "tensor_core")[0]
+    got, out, outw, conics = run_backward_path(cuda, case, gout, gw, path, mode)
+    sel = np.sort(rng.choice(means.shape[0], 20000, replace=False))
+    _, _, bb = orc.preprocess(means[sel], scales[sel], rots[sel], weights[sel])
+    g = orc.backward(means[sel], values[sel], weights[sel], conics[sel].astype(np.float64), bb, samples, out, outw,
+                     gout, gw)
+    ds, dq = orc.cov_backward(scales[sel], rots[sel], conics[sel], g["dconics"])
+    ref = [g["dmeans"], ds, dq, g["dvalues"].reshape(-1, 1), g["dweights"].reshape(-1, 1)]
     for k, name in enumerate(("means", "scales", "rots", "values", "weights")):
-        err = np.abs(b[k] - a[k]).max() / np.abs(a[k]).max()
-        print("%s: max err / max |plain| = %.2e" % (name, err))
+        a = got[k].reshape(means.shape[0], -1)[sel]
+        err = np.abs(a - ref[k]).max() / np.abs(ref[k]).max()
+        print("%s: max err / max |fp64| = %.2e" % (name, err))
         assert err <= (5e-4 if name in ("scales", "rots") else 1e-4), name

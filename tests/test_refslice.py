@@ -7,12 +7,14 @@ What this pins (tolerances written in each test):
     condition estimate stays under the FP64 threshold; AABB corners within 4 ulps of their
     addends (the oracle rounds m = sqrt(-2 ln(1e-3 / w)) once from double, the reference
     uses logf);
-  * the Gaussian-BVH forward (forward.cu:185-259): the reference's FP32 sums within
-    2e-6 relative of the oracle's FP64 sums over the same candidate set, identical
-    validity away from the 0.01 cutoff;
-  * the Gaussian-BVH backward (backward.cu:339-559): per-pair adjoint sums within 1e-5 of
-    max per field; the covariance adjoint (backward.cu:9-125) within 1e-5 of max against
-    the oracle's reference-compatible mode.
+  * the forward in both BVH modes (forward.cu:185-259 thread per sample; :116-182 and
+    :261-274 warp per Gaussian with atomic sums): the reference's FP32 sums within 2e-6
+    relative of the oracle's FP64 sums over the same candidate set, identical validity
+    away from the 0.01 cutoff;
+  * the backward in both modes (backward.cu:339-559 with atomic sums; :127-337 with warp
+    reductions): per-pair adjoint sums within 1e-5 of max per field; the covariance
+    adjoint (backward.cu:9-125) within 1e-5 of max against the oracle's
+    reference-compatible mode.
 """
 import os
 
@@ -82,8 +84,8 @@ def test_preprocess_fp64_switch_is_the_only_difference(orc, config1):
     assert rel(c32)[:64].max() < rel(rc)[:64].max()
 
 
-@pytest.mark.parametrize("which", ["config1", "trained"])
-def test_forward_matches_reference_code(orc, config1, which):
+@pytest.mark.parametrize("which,use_gaussian_bvh", [("config1", True), ("config1", False), ("trained", True)])
+def test_forward_matches_reference_code(orc, config1, which, use_gaussian_bvh):
     if which == "config1":
         means, scales, rots, values, weights, samples = config1
     else:
@@ -91,9 +93,16 @@ def test_forward_matches_reference_code(orc, config1, which):
         lo, hi = means.min(0), means.max(0)
         samples = (lo + np.random.default_rng(0).random((100000, 3)) * (hi - lo)).astype(np.float32)
     rc, rb = refslice.preprocess(means, scales, rots, weights)
-    out, outw, cnt = refslice.forward(means, values, weights, samples, rc, rb)
+    refslice.config(serial=True)
+    try:
+        out, outw, cnt = refslice.forward(means, values, weights, samples, rc, rb, use_gaussian_bvh=use_gaussian_bvh)
+    finally:
+        refslice.config(serial=False)
     ro, rw, rcnt = orc.forward(means, values, weights, rc.astype(np.float64), rb, samples, with_counts=True)
-    np.testing.assert_array_equal(cnt, rcnt)  # same contributing pairs per sample
+    if use_gaussian_bvh:
+        np.testing.assert_array_equal(cnt, rcnt)  # same contributing pairs per sample
+    else:
+        assert cnt.sum() == rcnt.sum()  # counted per Gaussian in this mode
     ok = np.abs(rw - 0.01) > 1e-6
     assert np.array_equal((out == -1)[ok], (ro == -1)[ok])
     v = ok & (ro != -1)
@@ -102,7 +111,8 @@ def test_forward_matches_reference_code(orc, config1, which):
     assert (np.abs(outw[v] - rw[v]) / rw[v]).max() <= 2e-6
 
 
-def test_backward_matches_reference_code(orc, config1):
+@pytest.mark.parametrize("use_gaussian_bvh", [True, False])
+def test_backward_matches_reference_code(orc, config1, use_gaussian_bvh):
     means, scales, rots, values, weights, samples = config1
     rc, rb = refslice.preprocess(means, scales, rots, weights)
     out, outw, _ = refslice.forward(means, values, weights, samples, rc, rb)
@@ -112,7 +122,8 @@ def test_backward_matches_reference_code(orc, config1):
     gw = (0.1 * rng.normal(size=S)).astype(np.float32)
     refslice.config(serial=True)
     try:
-        g = refslice.backward(means, scales, rots, rc, values, weights, rb, samples, out, outw, gout, gw)
+        g = refslice.backward(means, scales, rots, rc, values, weights, rb, samples, out, outw, gout, gw,
+                              use_gaussian_bvh=use_gaussian_bvh)
     finally:
         refslice.config(serial=False)
     go = orc.backward(means, values, weights, rc.astype(np.float64), rb, samples, out, outw, gout, gw)
