@@ -46,6 +46,10 @@ CONFIGS = {
     "tiny": (4_096, 262_144, "CPU-runnable case: 4096 clustered Gaussians x 64^3 points"),
     "config1": (4_096, 262_144, "small mixture: 4096 Gaussians (means U[0,1]^3, log-scales N(log 0.02, 0.3)) "
                                 "at the 64^3 cell centres"),
+    "config2": (200_000, 4_000_000, "structured-volume fit step: 256^3 volume (64 anisotropic blobs + "
+                                    "0.1 sin 8pi x sin 8pi y sin 8pi z), 200k Gaussians at random lattice points "
+                                    "(isotropic 3-NN scales, q = (1,0,0,0), w = 0.1, v = the volume there), 4M uniform "
+                                    "points, targets through gpu_sample"),
 }
 METRIC = "fwd+bwd ms/step (2M Gaussians×16M pts), TC vs plain FP32 at stated FP64 err"
 # Algorithmic FP32 work per pair (FORWARD forward.cu:224-256, BACKWARD backward.cu:252-298):
@@ -89,12 +93,48 @@ def parse():
     return p.parse_args()
 
 
+TARGETS = {}  # config -> target values of the workload's samples (configurations that define them)
+
+
+def config2_workload(P, S, seed=0):
+    """Config 2 as stated: the GaussianModel.create_from_pcd initialisation
+    (scene/gaussian_model.py:175-192: log-scale = log sqrt(max(distCUDA2, 1e-7)) on all
+    three axes, q = (1, 0, 0, 0), w = 0.1, v = the volume's value) activated by the
+    model's getters (:71-77, :114-132: exp + tanh soft cap at 0.02, normalise, identity for
+    the already activated w and v), S uniform points per step and their targets sampled
+    from the volume with gpu_sample (trilinear, as the training targets are made)."""
+    import torch
+    import gvc_workloads as wl
+    from gpu_mesh_sampling import gpu_sample
+    from simple_knn._C import distCUDA2
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n = 256
+    vol = wl.volume_blobs_sine(n=n, seed=seed, device=dev)
+    pts, vals = wl.lattice_init(vol, P, seed=seed)
+    s = torch.sqrt(torch.clamp_min(distCUDA2(pts), 1e-7))[:, None].repeat(1, 3)
+    r = torch.linalg.norm(s, dim=1, keepdim=True) + 1e-8
+    s = s * ((0.02 * torch.tanh(r / 0.02)) / r)
+    rots = torch.zeros(P, 4, device=dev)
+    rots[:, 0] = 1.0
+    g = torch.Generator(device="cpu").manual_seed(seed + 7)
+    samples = torch.rand(S, 3, generator=g).numpy()
+    target = gpu_sample(np.array([n, n, n]), np.zeros(3, np.float32), np.full(3, 1.0 / (n - 1), np.float32),
+                        vol.reshape(-1).cpu().numpy(), samples)
+    f = lambda t: np.ascontiguousarray(t.detach().cpu().numpy().astype(np.float32))
+    return (f(pts), f(s), f(rots), f(vals), np.full(P, 0.1, np.float32), samples.astype(np.float32),
+            np.ascontiguousarray(target.astype(np.float32)))
+
+
 def workload(cfg, rank):
     import gvc_workloads as wl
     P, S, desc = CONFIGS[cfg]
     if cfg == "config1":
         means, scales, rots, values, weights = wl.mixture_small(seed=0, P=P)
         return means, scales, rots, values, weights, wl.grid_centres(64), desc
+    if cfg == "config2":
+        means, scales, rots, values, weights, samples, target = config2_workload(P, S, seed=rank)
+        TARGETS[cfg] = target
+        return means, scales, rots, values, weights, samples, desc
     means, scales, rots, values, weights, _ = wl.mixture_large(seed=0, P=P, S=2)
     # per-rank sample set (weak scaling); rank 0 uses the config's own seed
     _, _, _, _, _, samples = wl.mixture_large(seed=0 if rank == 0 else 1000 + rank, P=P, S=S)
@@ -180,14 +220,18 @@ def cpu_kind():
     return "reference" if refslice.available() else "port"
 
 
-def cpu_step_time(kind, means, scales, rots, values, weights, samples, n_sub, seed=5):
+def cpu_step_time(kind, means, scales, rots, values, weights, samples, n_sub, seed=5, target=None):
     """One CPU step on n_sub of the points: preprocess, forward, masked-L1 gradient,
     backward (covariance adjoint included).  kind "reference": the reference's kernels in
     its default (sample-BVH) mode, FP32, all host threads; "port": the FP64 oracle."""
     _oracle_path()
     rng = np.random.default_rng(seed)
-    sub = samples[rng.choice(samples.shape[0], n_sub, replace=False)]
-    gt = (0.5 + 0.4 * np.sin(6 * sub[:, 0]) * np.sin(5 * sub[:, 1]) * np.sin(4 * sub[:, 2])).astype(np.float32)
+    pick = rng.choice(samples.shape[0], n_sub, replace=False)
+    sub = samples[pick]
+    if target is not None:
+        gt = target[pick]
+    else:
+        gt = (0.5 + 0.4 * np.sin(6 * sub[:, 0]) * np.sin(5 * sub[:, 1]) * np.sin(4 * sub[:, 2])).astype(np.float32)
     t0 = time.perf_counter()
     if kind == "reference":
         import refslice
@@ -221,10 +265,12 @@ def cpu_extrapolated(kind, means, scales, rots, values, weights, samples, n_a, n
     n_b runs; extrapolates t = fixed + slope * S to the full step."""
     threads = os.cpu_count() or 1
     S = samples.shape[0]
-    t_a = cpu_step_time(kind, means, scales, rots, values, weights, samples, n_a)
+    tg = TARGETS.get("config2") if means.shape[0] == CONFIGS["config2"][0] and S == CONFIGS["config2"][1] else None
+    t_a = cpu_step_time(kind, means, scales, rots, values, weights, samples, n_a, target=tg)
     for _ in range(warmup):
-        cpu_step_time(kind, means, scales, rots, values, weights, samples, n_b)
-    tb = [cpu_step_time(kind, means, scales, rots, values, weights, samples, n_b, seed=10 + k) for k in range(reps_b)]
+        cpu_step_time(kind, means, scales, rots, values, weights, samples, n_b, target=tg)
+    tb = [cpu_step_time(kind, means, scales, rots, values, weights, samples, n_b, seed=10 + k, target=tg)
+          for k in range(reps_b)]
     t_b = float(np.median(tb))
     slope = (t_b - t_a) / (n_b - n_a)
     fixed = max(t_a - slope * n_a, 0.0)
@@ -520,7 +566,7 @@ def run_ours(args):
     P, S = means.shape[0], samples.shape[0]
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     d_means, d_scales, d_rots, d_values, d_weights, d_samples = map(T, (means, scales, rots, values, weights, samples))
-    d_gt = target_field(d_samples)
+    d_gt = T(TARGETS[args.config]) if args.config in TARGETS else target_field(d_samples)
     zeros_w = torch.zeros(S, device=dev)
     ugb = bool(args.use_gaussian_bvh)
     _C.set_backward_mode(args.bwd_mode)
@@ -617,7 +663,8 @@ def run_ours(args):
         h_samples = torch.from_numpy(samples).pin_memory()
         # the target values travel with their samples, as the training loop's sorted
         # (samples, ground truth) batches do (train.py:286-315)
-        h_gt = target_field(torch.from_numpy(samples)).pin_memory()
+        h_gt = (torch.from_numpy(TARGETS[args.config]) if args.config in TARGETS else
+                target_field(torch.from_numpy(samples))).pin_memory()
         h_params = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
                     for a in (means, scales, rots, values.reshape(-1, 1), weights.reshape(-1, 1))]
         settings = R.GaussianRasterizationSettings((0, 0, 0), (1, 1, 1), 0, -1.0, 1.0, ugb, False)

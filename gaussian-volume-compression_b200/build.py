@@ -27,6 +27,7 @@ SOURCES = {
     "mesh.cu": ["--fmad=false"],
     "noalloc.cu": [],
     "cta.cu": [],
+    "fwd_tc.cu": [],
     "bwd_tc.cu": [],
     "knn.cu": [],
     "trainsamp.cu": [],

@@ -71,6 +71,8 @@ cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32
                                  float4* bboxes, float ratio, cudaStream_t st, uint2* bdesc2 = nullptr,
                                  float4* bboxes2 = nullptr, float ratio2 = 0.f);
 cudaError_t launch_forward_cta(const CtaArgs& a, bool tc, cudaStream_t st);
+// fwd_tc.cu: the forward with the exponent on tcgen05 (launch_forward_cta(a, true) calls it)
+cudaError_t launch_forward_tc(const CtaArgs& a, cudaStream_t st);
 cudaError_t launch_tc_gemm_test(const void* A, const void* B, int N, float* D, int* status, cudaStream_t st);
 cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st);
 // bwd_tc.cu: backward on 128-sample blocks with the reduction over samples on tcgen05

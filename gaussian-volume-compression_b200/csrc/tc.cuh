@@ -174,4 +174,50 @@ __device__ __forceinline__ void split_bf16(const float (&v)[16], __nv_bfloat16 (
     }
 }
 
+// ---- split-BF16 operand rows and narrower TMEM reads ------------------------------------
+__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
+
+// Splits (a, b) into three BF16 parts each: a = h.x + m.x + l.x (~24 bits), same for b.
+__device__ __forceinline__ void split3_pair(float a, float b, uint32_t& h, uint32_t& m, uint32_t& l) {
+    const __nv_bfloat162 H = __floats2bfloat162_rn(a, b);
+    const float ra = a - __low2float(H), rb = b - __high2float(H);
+    const __nv_bfloat162 M = __floats2bfloat162_rn(ra, rb);
+    const float sa = ra - __low2float(M), sb = rb - __high2float(M);
+    const __nv_bfloat162 L = __floats2bfloat162_rn(sa, sb);
+    h = bf2_bits(H);
+    m = bf2_bits(M);
+    l = bf2_bits(L);
+}
+
+// Writes the ten features f[0..9] of row r into the three parts of a K-major no-swizzle
+// tile (element (r, k) at (r / 8) * 256 + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2);
+// features 10..15 are left as they are (zero).
+__device__ __forceinline__ void store_features10(unsigned char* t0, unsigned char* t1, unsigned char* t2, int r,
+                                                 const float (&f)[10]) {
+    uint32_t h[5], m[5], l[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) split3_pair(f[2 * i], f[2 * i + 1], h[i], m[i], l[i]);
+    const int off = (r >> 3) * 256 + (r & 7) * 16;
+    *reinterpret_cast<uint4*>(t0 + off) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(t1 + off) = make_uint4(m[0], m[1], m[2], m[3]);
+    *reinterpret_cast<uint4*>(t2 + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    *reinterpret_cast<uint32_t*>(t0 + off + 128) = h[4];
+    *reinterpret_cast<uint32_t*>(t1 + off + 128) = m[4];
+    *reinterpret_cast<uint32_t*>(t2 + off + 128) = l[4];
+}
+
+// Warp-wide: thread t receives columns [col, col + 16) of TMEM lane (lane base + t).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
 }  // namespace gvc

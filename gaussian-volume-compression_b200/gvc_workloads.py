@@ -59,6 +59,56 @@ def mixture_large(seed=0, P=2_000_000, S=16_000_000):
     return means, scales, q, values, weights, samples
 
 
+def volume_blobs_sine(n=256, seed=0, nblobs=64, device="cpu"):
+    """Config 2 volume: an n^3 float32 point field on the lattice i / (n - 1) of [0,1]^3
+    (x fastest), the sum of `nblobs` random anisotropic Gaussian blobs (centres U[0,1]^3,
+    standard deviations U[0.03, 0.1] per axis, random rotation, amplitude U[0.5, 1]) plus
+    0.1 sin(8 pi x) sin(8 pi y) sin(8 pi z), mapped linearly onto [0.01, 0.99] (the
+    values initialise Gaussian values through the inverse sigmoid, so they must stay
+    inside (0, 1)).  Computed with torch on `device` (a CUDA device makes 256^3 fast)."""
+    import torch
+    rng = np.random.default_rng(seed + 2000)
+    c = torch.tensor(rng.random((nblobs, 3)), dtype=torch.float32, device=device)
+    sd = rng.uniform(0.03, 0.1, (nblobs, 3))
+    q = rng.normal(size=(nblobs, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    r, x, y, z = q.T
+    R = np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - r * z), 2 * (x * z + r * y)], -1),
+                  np.stack([2 * (x * y + r * z), 1 - 2 * (x * x + z * z), 2 * (y * z - r * x)], -1),
+                  np.stack([2 * (x * z - r * y), 2 * (y * z + r * x), 1 - 2 * (x * x + y * y)], -1)], -2)
+    prec = np.einsum("bij,bj,bkj->bik", R, 1.0 / sd ** 2, R)  # Sigma^-1 = R diag(1/s^2) R^T
+    prec = torch.tensor(prec, dtype=torch.float32, device=device)
+    amp = torch.tensor(rng.uniform(0.5, 1.0, nblobs), dtype=torch.float32, device=device)
+    t = torch.arange(n, dtype=torch.float32, device=device) / (n - 1)
+    out = torch.empty(n, n, n, dtype=torch.float32, device=device)  # [z][y][x]
+    zz, yy, xx = torch.meshgrid(t, t, t, indexing="ij")
+    pts = torch.stack([xx, yy, zz], -1).reshape(-1, 3)
+    acc = torch.zeros(pts.shape[0], dtype=torch.float32, device=device)
+    chunk = 1 << 21
+    for a in range(0, pts.shape[0], chunk):
+        p = pts[a:a + chunk]
+        for b in range(nblobs):
+            d = p - c[b]
+            acc[a:a + chunk] += amp[b] * torch.exp(-0.5 * ((d @ prec[b]) * d).sum(-1))
+    acc += 0.1 * torch.sin(8 * np.pi * pts[:, 0]) * torch.sin(8 * np.pi * pts[:, 1]) * torch.sin(8 * np.pi * pts[:, 2])
+    lo, hi = acc.min(), acc.max()
+    out = (0.01 + 0.98 * (acc - lo) / (hi - lo)).reshape(n, n, n)
+    return out
+
+
+def lattice_init(volume, P, seed=0):
+    """Config 2 initial mixture positions: P distinct random lattice points of the volume
+    (its voxel centres on [0,1]^3) and the volume's values there; returns (points [P,3]
+    float32, values [P] float32) on the volume's device."""
+    import torch
+    n = volume.shape[0]
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    idx = torch.randperm(n ** 3, generator=g)[:P].to(volume.device)
+    x, y, z = idx % n, (idx // n) % n, idx // (n * n)
+    pts = torch.stack([x, y, z], 1).float() / (n - 1)
+    return pts.contiguous(), volume.reshape(-1)[idx].contiguous()
+
+
 def jittered_tet_mesh(n=16, seed=0, jitter=0.2):
     """Config 3 geometry: an n^3 hex grid on [0,1]^3, interior vertices jittered by
     U[-jitter, jitter]*h, each hex split into 6 tets along its main diagonal (Kuhn
