@@ -96,6 +96,32 @@ def volume_blobs_sine(n=256, seed=0, nblobs=64, device="cpu"):
     return out
 
 
+def volume_turbulent(n=512, seed=0, modes=256, kmax=32, device="cpu"):
+    """Config 5 volume: an n^3 float32 point field on the lattice i / (n - 1) of [0,1]^3
+    (x fastest), a spectral sum of `modes` random Fourier modes
+    sum_m |k_m|^(-5/3) cos(2 pi k_m . x + phi_m) with integer wave vectors k_m uniform in
+    [-kmax, kmax]^3 other than 0 and phases U[0, 2 pi), normalised to [0, 1]."""
+    import torch
+    rng = np.random.default_rng(seed + 3000)
+    k = rng.integers(-kmax, kmax + 1, (modes, 3))
+    k[np.all(k == 0, axis=1)] = [1, 0, 0]
+    amp = np.linalg.norm(k, axis=1) ** (-5.0 / 3.0)
+    phi = rng.uniform(0, 2 * np.pi, modes)
+    K = torch.tensor(2 * np.pi * k, dtype=torch.float32, device=device)
+    A = torch.tensor(amp, dtype=torch.float32, device=device)
+    Ph = torch.tensor(phi, dtype=torch.float32, device=device)
+    t = torch.arange(n, dtype=torch.float32, device=device) / (n - 1)
+    out = torch.empty(n ** 3, dtype=torch.float32, device=device)
+    plane = n * n
+    yy, xx = torch.meshgrid(t, t, indexing="ij")
+    xy = torch.stack([xx.reshape(-1), yy.reshape(-1)], 1)
+    for z in range(n):
+        p = torch.cat([xy, torch.full((plane, 1), float(t[z]), device=device)], 1)
+        out[z * plane:(z + 1) * plane] = torch.cos(p @ K.T + Ph) @ A
+    lo, hi = out.min(), out.max()
+    return ((out - lo) / (hi - lo)).reshape(n, n, n)
+
+
 def lattice_init(volume, P, seed=0):
     """Config 2 initial mixture positions: P distinct random lattice points of the volume
     (its voxel centres on [0,1]^3) and the volume's values there; returns (points [P,3]
