@@ -35,7 +35,8 @@ constexpr int kMom = 32;               // B rows: 20 moment features + zero padd
 struct BwdSmem {
     unsigned char A[2][2][kBBatch * 32];        // E chunk (128 x 16 bf16), two parts, two buffers
     unsigned char B[kBChunks][3][kMom * 32];    // Psi (32 x 16 bf16) per chunk, three parts
-    float4 rows[kBRows];                        // (x, y, z, W > 0.01) of the block's rows
+    float rx[kBRows], ry[kBRows], rz[kBRows];  // coordinates of the block's rows (pairs load as float2)
+    uint8_t rok[kBRows];                        // W > 0.01 (pair statistics only)
     int cand[kBStages][kBBatch];                // candidate Gaussians (LBVH leaf = record index)
     int2 desc[kBStages];                        // (count or -1 at the end, group)
     int stack[kStackCap];
@@ -139,7 +140,10 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
             const float4 q = s_grad[row];
             p = make_float4(q.x, q.y, q.z, s_ok[row] ? 1.f : 0.f);
         }
-        sm.rows[t] = p;
+        sm.rx[t] = p.x;
+        sm.ry[t] = p.y;
+        sm.rz[t] = p.z;
+        sm.rok[t] = p.w != 0.f;
     }
     if (w == 0) {
         static_assert(tmem_cols_ok(kMom), "TMEM columns must be a power of two >= 32");
@@ -279,6 +283,10 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 bhi = __ldg(rp + 4);
             }
             const GaussB g = gauss_b(r0.x, r0.y, r0.z, r2.z, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, blo, bhi);
+            const float2 nmx = make_float2(-g.mx, -g.mx), nmy = make_float2(-g.my, -g.my),
+                         nmz = make_float2(-g.mz, -g.mz);
+            const float2 Q0 = make_float2(g.q0, g.q0), Q1 = make_float2(g.q1, g.q1), Q2 = make_float2(g.q2, g.q2),
+                         Q3 = make_float2(g.q3, g.q3), Q4 = make_float2(g.q4, g.q4), Q5 = make_float2(g.q5, g.q5);
             bool okc = true;
             for (int q = q0; q <= q1; q++, j++) {
                 const int b = (int)(j & 1u);
@@ -294,35 +302,47 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 // rows of the chunk inside the group (warp-uniform bit mask)
                 const int c0 = max(ra - 16 * q, 0), c1 = min(rb - 16 * q, 16);
                 const uint32_t rmask = c1 > c0 ? (((1u << (c1 - c0)) - 1u) << c0) : 0u;
-                float e[16];
+                // Rows two at a time: the coordinates load as float2 pairs and the power runs
+                // on packed f32x2 FMAs (the AABB test, window and ex2 per row).
+                uint32_t hw[8], mw[8];
 #pragma unroll
-                for (int k = 0; k < 16; k++) {
+                for (int k = 0; k < 16; k += 2) {
                     const int r = 16 * q + k;
-                    const float4 p = sm.rows[r];
-                    const bool in = ((rmask >> k) & 1u) && g.lx <= p.x && p.x <= g.hx && g.ly <= p.y && p.y <= g.hy &&
-                                    g.lz <= p.z && p.z <= g.hz;
-                    const float dx = p.x - g.mx, dy = p.y - g.my, dz = p.z - g.mz;
-                    const float p2 = dx * fmaf(g.q0, dx, fmaf(g.q1, dy, g.q2 * dz)) +
-                                     dy * fmaf(g.q3, dy, g.q4 * dz) + dz * (g.q5 * dz);
-                    const bool c = in && p2 >= kLog2Floor && p2 <= 0.0f;
-                    e[k] = c ? ex2_approx(p2) : 0.f;
+                    const float2 X = *reinterpret_cast<const float2*>(&sm.rx[r]);
+                    const float2 Y = *reinterpret_cast<const float2*>(&sm.ry[r]);
+                    const float2 Z = *reinterpret_cast<const float2*>(&sm.rz[r]);
+                    const bool in0 = ((rmask >> k) & 1u) && g.lx <= X.x && X.x <= g.hx && g.ly <= Y.x && Y.x <= g.hy &&
+                                     g.lz <= Z.x && Z.x <= g.hz;
+                    const bool in1 = ((rmask >> (k + 1)) & 1u) && g.lx <= X.y && X.y <= g.hx && g.ly <= Y.y &&
+                                     Y.y <= g.hy && g.lz <= Z.y && Z.y <= g.hz;
+                    const float2 dX = __fadd2_rn(X, nmx), dY = __fadd2_rn(Y, nmy), dZ = __fadd2_rn(Z, nmz);
+                    // p2 = dx (q0 dx + q1 dy + q2 dz) + dy (q3 dy + q4 dz) + dz (q5 dz)
+                    float2 a = __ffma2_rn(Q0, dX, __ffma2_rn(Q1, dY, __fmul2_rn(Q2, dZ)));
+                    a = __fmul2_rn(dX, a);
+                    a = __ffma2_rn(dY, __ffma2_rn(Q3, dY, __fmul2_rn(Q4, dZ)), a);
+                    const float2 P2 = __ffma2_rn(dZ, __fmul2_rn(Q5, dZ), a);
+                    const bool c0 = in0 && P2.x >= kLog2Floor && P2.x <= 0.0f;
+                    const bool c1 = in1 && P2.y >= kLog2Floor && P2.y <= 0.0f;
+                    const float e0 = c0 ? ex2_approx(P2.x) : 0.f, e1 = c1 ? ex2_approx(P2.y) : 0.f;
+                    // E in two BF16 parts (~16 bits: e to 2^-16 relative); Psi keeps three
+                    const __nv_bfloat162 H = __floats2bfloat162_rn(e0, e1);
+                    const __nv_bfloat162 M = __floats2bfloat162_rn(e0 - __low2float(H), e1 - __high2float(H));
+                    hw[k >> 1] = *reinterpret_cast<const uint32_t*>(&H);
+                    mw[k >> 1] = *reinterpret_cast<const uint32_t*>(&M);
                     if (COUNT) {
-                        ncand += in ? 1 : 0;
-                        ncontrib += (c && p.w != 0.f) ? 1 : 0;
-                        nlane += 32;
+                        ncand += (in0 ? 1 : 0) + (in1 ? 1 : 0);
+                        ncontrib += ((c0 && sm.rok[r]) ? 1 : 0) + ((c1 && sm.rok[r + 1]) ? 1 : 0);
+                        nlane += 64;
                     }
                 }
                 tc_fence_after();
                 {
-                    // E in two BF16 parts (~16 bits: e to 2^-16 relative); Psi keeps three
-                    __nv_bfloat16 h[16], m[16];
-#pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        h[i] = __float2bfloat16_rn(e[i]);
-                        m[i] = __float2bfloat16_rn(e[i] - __bfloat162float(h[i]));
-                    }
-                    store_row_k16(sm.A[b][0], t, h);
-                    store_row_k16(sm.A[b][1], t, m);
+                    unsigned char* a0 = sm.A[b][0] + (t >> 3) * 256 + (t & 7) * 16;
+                    unsigned char* a1 = sm.A[b][1] + (t >> 3) * 256 + (t & 7) * 16;
+                    *reinterpret_cast<uint4*>(a0) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    *reinterpret_cast<uint4*>(a0 + 128) = make_uint4(hw[4], hw[5], hw[6], hw[7]);
+                    *reinterpret_cast<uint4*>(a1) = make_uint4(mw[0], mw[1], mw[2], mw[3]);
+                    *reinterpret_cast<uint4*>(a1 + 128) = make_uint4(mw[4], mw[5], mw[6], mw[7]);
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
