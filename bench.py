@@ -83,6 +83,8 @@ def parse():
     # deterministic one ("auto"), timed beside it in tc_vs_plain
     p.add_argument("--bwd-mode", default="tensor_core", choices=["auto", "deterministic", "atomic", "tensor_core"])
     p.add_argument("--eval-path", default="plain", choices=["plain", "tensor_core", "plain_tile"])
+    p.add_argument("--traversal", default="stack", choices=["stack", "stackless"],
+                   help="Gaussian-LBVH traversal of the block-group kernels (both are timed in tc_vs_plain)")
     p.add_argument("--use-gaussian-bvh", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -373,7 +375,7 @@ def grad_errors(means, scales, rots, values, weights, samples, runs, n_gauss=10_
 def config_dict(args, desc, P, S, world):
     """The config object of both arms' lines (identical for the same arguments)."""
     return {"workload": desc, "P": P, "S_per_gpu": S, "path": args.eval_path, "backward": args.bwd_mode,
-            "use_gaussian_bvh": bool(args.use_gaussian_bvh),
+            "traversal": args.traversal, "use_gaussian_bvh": bool(args.use_gaussian_bvh),
             "l2": "inputs larger than L2 (samples %d MB, Gaussian records %d MB)" % (S * 12 // 2**20, P * 80 // 2**20),
             "parallelism": "samples sharded per rank, NCCL all-reduce of gradients" if world > 1 else "single GPU"}
 
@@ -758,6 +760,7 @@ def run_ours(args):
     ugb = bool(args.use_gaussian_bvh)
     _C.set_backward_mode(args.bwd_mode)
     _C.set_eval_path(args.eval_path)
+    _C.set_traversal(args.traversal)
     bounds = (0.0, 0.0, 0.0, 1.0, 1.0, 1.0)
 
     def step():
@@ -944,12 +947,16 @@ def run_ours(args):
     grad_runs = {}
     paths_extra = {}
     if not args.profile:
-        # (forward path, backward mode): FP32 throughout, tensor cores throughout, and the FP32
-        # forward with the tensor-core backward reduction
-        for name, path, bmode in (("plain", "plain", "auto"), ("tensor_core", "tensor_core", "auto"),
-                                  ("plain_fwd_tc_bwd", "plain", "tensor_core")):
+        # (forward path, backward mode, traversal): FP32 throughout, tensor cores throughout, the
+        # FP32 forward with the tensor-core backward reduction, and that with the stackless
+        # Gaussian-LBVH traversal (timed only)
+        for name, path, bmode, trav in (("plain", "plain", "auto", "stack"),
+                                        ("tensor_core", "tensor_core", "auto", "stack"),
+                                        ("plain_fwd_tc_bwd", "plain", "tensor_core", "stack"),
+                                        ("stackless", "plain", "tensor_core", "stackless")):
             _C.set_eval_path(path)
             _C.set_backward_mode(bmode)
+            _C.set_traversal(trav)
             for _ in range(2):
                 step()
             torch.cuda.synchronize()
@@ -962,6 +969,9 @@ def run_ours(args):
             b1.record(stream)
             torch.cuda.synchronize()
             pm = gvc_dist.max_over_ranks(b0.elapsed_time(b1) / args.steps, dev)
+            if name == "stackless":
+                paths_extra["plain_fwd_tc_bwd_stackless_ms_per_step"] = pm
+                continue
             # one more step, outputs and gradients kept (untimed)
             _C.build_bvh(d_samples, False, ugb)
             o, ow, cn = _C.rasterize_gaussians(d_means, d_scales, d_rots, d_values, d_weights, 1.0, *bounds, -1.0,
@@ -976,11 +986,12 @@ def run_ours(args):
                    "grads": [x.cpu().numpy() for x in gr]}
             grad_runs[name] = run
             if name == "plain_fwd_tc_bwd":
-                paths_extra = {"plain_fwd_tc_bwd_ms_per_step": pm}
+                paths_extra["plain_fwd_tc_bwd_ms_per_step"] = pm
                 continue
             paths[name] = run
         _C.set_eval_path(args.eval_path)
         _C.set_backward_mode(args.bwd_mode)
+        _C.set_traversal(args.traversal)
         _C.check_status()
 
     cpu = None
@@ -996,7 +1007,9 @@ def run_ours(args):
                        "speedup_tc_over_plain": paths["plain"]["ms_per_step"] / paths["tensor_core"]["ms_per_step"],
                        "paths": {"plain": "FP32 CTA forward + FP32 deterministic Gaussian-owned backward",
                                  "tensor_core": "tcgen05 split-BF16 exponent forward + tcgen05 moment backward",
-                                 "plain_fwd_tc_bwd": "FP32 CTA forward + tcgen05 moment backward"},
+                                 "plain_fwd_tc_bwd": "FP32 CTA forward + tcgen05 moment backward",
+                                 "plain_fwd_tc_bwd_stackless": "the same with the stackless Gaussian-LBVH "
+                                                               "traversal (escape edges) in both kernels"},
                        "fp64_error": fp64}
         tc_vs_plain.update(paths_extra)
 

@@ -196,6 +196,13 @@ def set_eval_path(path, device=None):
     set_option(_n.OPT_EVAL_PATH, {"plain": 0, "tensor_core": 1, "plain_tile": 2}[path], device)
 
 
+def set_traversal(kind, device=None):
+    """Gaussian-LBVH traversal of the block-group forwards and the tensor-core backward:
+    'stack' (default: warp-cooperative, shared-memory node stack) or 'stackless' (escape
+    edges, one subtree per lane below the levels that fit the warp).  Same candidates."""
+    set_option(_n.OPT_TRAVERSAL, {"stack": 0, "stackless": 1}[kind], device)
+
+
 def set_count_pairs(on, device=None):
     set_option(_n.OPT_COUNT_PAIRS, 1 if on else 0, device)
 

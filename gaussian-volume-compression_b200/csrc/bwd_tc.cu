@@ -104,10 +104,11 @@ __device__ __forceinline__ void store_split_row(unsigned char* t0, unsigned char
     store_row_k16(t2, r, l);
 }
 
-template <bool COUNT>
+template <bool COUNT, bool STACKLESS>
 __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     int64_t n_slots, const uint2* __restrict__ bdesc, const float4* __restrict__ bboxes,
-    const BvhNode* __restrict__ gnodes, const GaussRec* __restrict__ recs, const int32_t* __restrict__ gperm,
+    const BvhNode* __restrict__ gnodes, int64_t n_internal, const GaussRec* __restrict__ recs,
+    const int32_t* __restrict__ gperm,
     const float4* __restrict__ s_grad, const float* __restrict__ s_gyz, const uint8_t* __restrict__ s_ok,
     float* __restrict__ gacc, int* status, unsigned long long* stats) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -163,8 +164,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
         for (int g = 0; g < ng && !pr.failed; g++) {
             pr.g = g;
             const float4 glo = bboxes[2 * (blk * kBGroups + g)], ghi = bboxes[2 * (blk * kBGroups + g) + 1];
-            st |= warp_traverse(gnodes, make_float3(glo.x, glo.y, glo.z), make_float3(ghi.x, ghi.y, ghi.z), sm.stack,
-                                sm.tcand, pr, tc);
+            st |= warp_traverse_sel<STACKLESS>(gnodes, n_internal, make_float3(glo.x, glo.y, glo.z),
+                                               make_float3(ghi.x, ghi.y, ghi.z), sm.stack, sm.tcand, pr, tc);
             if (pr.fill > 0 && !pr.failed) pr.publish(pr.fill);
         }
         if (lane == 0) {
@@ -409,15 +410,16 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     if (w == 0) tmem_dealloc(tmem, kMom);
 }
 
-template <bool COUNT>
+template <bool COUNT, bool STACKLESS>
 static cudaError_t launch_bwd_cta_impl(const BwdArgs& a, int64_t n_blocks, const uint2* bdesc, const float4* bboxes,
                                        cudaStream_t st) {
     const size_t smem = sizeof(BwdSmem) + 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_backward_cta<COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_backward_cta<COUNT, STACKLESS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_backward_cta<COUNT><<<(unsigned)n_blocks, kBRows + 64, smem, st>>>(
-        a.n_tiles * kTile, bdesc, bboxes, a.gnodes, a.recs, a.gperm, a.s_grad, a.s_gyz, a.s_ok, a.gacc, a.status,
-        a.stats);
+    k_backward_cta<COUNT, STACKLESS><<<(unsigned)n_blocks, kBRows + 64, smem, st>>>(
+        a.n_tiles * kTile, bdesc, bboxes, a.gnodes, a.g_internal, a.recs, a.gperm, a.s_grad, a.s_gyz, a.s_ok,
+        a.gacc, a.status, a.stats);
     gvc::note_launch();
     return cudaGetLastError();
 }
@@ -425,8 +427,11 @@ static cudaError_t launch_bwd_cta_impl(const BwdArgs& a, int64_t n_blocks, const
 cudaError_t launch_backward_cta(const BwdArgs& a, int64_t n_blocks, const uint2* bdesc, const float4* bboxes,
                                 cudaStream_t st) {
     if (n_blocks <= 0 || a.P <= 0) return cudaSuccess;
-    return a.count ? launch_bwd_cta_impl<true>(a, n_blocks, bdesc, bboxes, st)
-                   : launch_bwd_cta_impl<false>(a, n_blocks, bdesc, bboxes, st);
+    if (a.stackless)
+        return a.count ? launch_bwd_cta_impl<true, true>(a, n_blocks, bdesc, bboxes, st)
+                       : launch_bwd_cta_impl<false, true>(a, n_blocks, bdesc, bboxes, st);
+    return a.count ? launch_bwd_cta_impl<true, false>(a, n_blocks, bdesc, bboxes, st)
+                   : launch_bwd_cta_impl<false, false>(a, n_blocks, bdesc, bboxes, st);
 }
 
 }  // namespace gvc

@@ -56,6 +56,13 @@ __global__ void k_boxes6_to_f4(int64_t n, const float* __restrict__ b6, float4* 
     out[2 * i + 1] = make_float4(b6[6 * i + 3], b6[6 * i + 4], b6[6 * i + 5], 0.f);
 }
 
+// escape edges of the stackless traversal (BvhNode c.w)
+__global__ void k_node_escape(int64_t n, const BvhNode* __restrict__ nodes, int32_t* __restrict__ out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = __float_as_int(nodes[i].c.w);
+}
+
 __global__ void k_f4_to_boxes6(int64_t n, const float4* __restrict__ in, float* __restrict__ b6) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -218,6 +225,10 @@ int gvc_set_option(gvc_ctx* ctx, int option, int value) {
         case GVC_OPT_COUNT_PAIRS:
             ctx->count_pairs = value ? 1 : 0;
             return GVC_OK;
+        case GVC_OPT_TRAVERSAL:
+            if (value < 0 || value > 1) return fail(ctx, GVC_ERR_ARG, "traversal must be 0 or 1");
+            ctx->traversal = value;
+            return GVC_OK;
         case GVC_OPT_TIME_KERNELS:
             drain_events(ctx);
             ctx->time_kernels = value ? 1 : 0;
@@ -378,7 +389,7 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
         const int rc = ensure_tile_groups(ctx, st);
         if (rc != GVC_OK) return rc;
     }
-    FwdArgs fa;
+    FwdArgs fa{};
     fa.s_sorted = ctx->s_sorted.as<float4>();
     fa.tile_boxes = ctx->tile_boxes.as<float4>();
     fa.gdesc = ctx->tile_gdesc.as<uint32_t>();
@@ -394,12 +405,14 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
     if (ctx->eval_path == 2) {
         GVC_CUDA(launch_forward(fa, st), "forward");
     } else {
-        CtaArgs ca;
+        CtaArgs ca{};
         ca.s_sorted = ctx->s_sorted.as<float4>();
         ca.S = ctx->S;
         ca.bdesc = ctx->blk_desc.as<uint2>();
         ca.bboxes = ctx->blk_boxes.as<float4>();
         ca.gnodes = ctx->gbvh.nodes.as<BvhNode>();
+        ca.n_internal = ctx->gbvh.n > 1 ? ctx->gbvh.n - 1 : 1;
+        ca.stackless = ctx->traversal == 1;
         ca.recs = ctx->grec.as<GaussRec>();
         ca.out_cells = out_cells;
         ca.out_weights = out_weights;
@@ -465,7 +478,7 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
                                      dL_dout_weights, ctx->s_grad.as<float4>(), ctx->s_gyz.as<float>(),
                                      ctx->s_ok.as<uint8_t>(), st),
                  "sample grads");
-        BwdArgs ba;
+        BwdArgs ba{};
         ba.P = P;
         ba.means = means3D;
         ba.values = values;
@@ -500,6 +513,8 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
             ba.gorder = nullptr;
             ba.gperm = ctx->gbvh.perm.as<int32_t>();
             ba.gnodes = ctx->gbvh.nodes.as<BvhNode>();
+            ba.g_internal = ctx->gbvh.n > 1 ? ctx->gbvh.n - 1 : 1;
+            ba.stackless = ctx->traversal == 1;
             ba.recs = ctx->grec.as<GaussRec>();
             const int tk = timer_begin(ctx, st, 1);
             const int64_t n_blocks = (S + 127) / 128;
@@ -707,6 +722,18 @@ int gvc_debug_lbvh(gvc_ctx* ctx, int64_t n, const float* boxes, uint32_t* keys_s
         if (node_boxes) k_f4_to_boxes6<<<nb(n - 1, 256), 256, 0, st>>>(n - 1, sc->dbg.node_boxes.as<float4>(), node_boxes); gvc::note_launch();
     }
     GVC_CUDA(cudaGetLastError(), "debug lbvh");
+    return GVC_OK;
+}
+
+int gvc_debug_lbvh_escape(gvc_ctx* ctx, int32_t* escape, void* stream) {
+    if (!ctx || !escape) return GVC_ERR_ARG;
+    Scratch* sc = scratch_of(ctx);
+    const int64_t n = sc->dbg.n;
+    if (n <= 0) return fail(ctx, GVC_ERR_STATE, "gvc_debug_lbvh has not built a tree");
+    const int64_t ni = n > 1 ? n - 1 : 1;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_node_escape<<<nb(ni, 256), 256, 0, st>>>(ni, sc->dbg.nodes.as<BvhNode>(), escape); gvc::note_launch();
+    GVC_CUDA(cudaGetLastError(), "debug lbvh escape");
     return GVC_OK;
 }
 

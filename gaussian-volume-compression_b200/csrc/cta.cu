@@ -342,10 +342,10 @@ struct Producer {
     }
 };
 
-template <bool COUNT>
+template <bool COUNT, bool STACKLESS>
 __global__ void __launch_bounds__(kConsumerWarps * 32 + 32, kCtaMinBlocks)
     k_forward_cta(const float4* __restrict__ s_sorted, int64_t S, const uint2* __restrict__ bdesc,
-                  const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes,
+                  const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes, int64_t n_internal,
                   const GaussRec* __restrict__ recs, float* __restrict__ out_cells, float* __restrict__ out_weights,
                   int* status, unsigned long long* stats) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -401,8 +401,8 @@ __global__ void __launch_bounds__(kConsumerWarps * 32 + 32, kCtaMinBlocks)
                 }
             }
             __syncwarp();
-            st |= warp_traverse(nodes, make_float3(glo.x, glo.y, glo.z), make_float3(ghi.x, ghi.y, ghi.z), sm.stack,
-                                sm.cand, pr, tc);
+            st |= warp_traverse_sel<STACKLESS>(nodes, n_internal, make_float3(glo.x, glo.y, glo.z),
+                                               make_float3(ghi.x, ghi.y, ghi.z), sm.stack, sm.cand, pr, tc);
         }
         pr.flush();
         if (st && lane == 0) atomicOr(status, st);
@@ -538,13 +538,15 @@ cudaError_t launch_sample_blocks(int64_t S, const float4* s_sorted, const uint32
     return cudaGetLastError();
 }
 
-template <bool COUNT>
+template <bool COUNT, bool STACKLESS>
 static cudaError_t launch_cta_impl(const CtaArgs& a, cudaStream_t st) {
     const size_t smem = sizeof(CtaSmem);
-    cudaError_t e = cudaFuncSetAttribute(k_forward_cta<COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_forward_cta<COUNT, STACKLESS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_forward_cta<COUNT><<<nblk128(a.S), kConsumerWarps * 32 + 32, smem, st>>>(
-        a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.recs, a.out_cells, a.out_weights, a.status, a.stats);
+    k_forward_cta<COUNT, STACKLESS><<<nblk128(a.S), kConsumerWarps * 32 + 32, smem, st>>>(
+        a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.n_internal, a.recs, a.out_cells, a.out_weights, a.status,
+        a.stats);
     gvc::note_launch();
     return cudaGetLastError();
 }
@@ -552,7 +554,8 @@ static cudaError_t launch_cta_impl(const CtaArgs& a, cudaStream_t st) {
 cudaError_t launch_forward_cta(const CtaArgs& a, bool tc, cudaStream_t st) {
     if (a.S <= 0) return cudaSuccess;
     if (tc) return launch_forward_tc(a, st);
-    return a.count ? launch_cta_impl<true>(a, st) : launch_cta_impl<false>(a, st);
+    if (a.stackless) return a.count ? launch_cta_impl<true, true>(a, st) : launch_cta_impl<false, true>(a, st);
+    return a.count ? launch_cta_impl<true, false>(a, st) : launch_cta_impl<false, false>(a, st);
 }
 
 cudaError_t launch_tc_gemm_test(const void* A, const void* B, int N, float* D, int* status, cudaStream_t st) {

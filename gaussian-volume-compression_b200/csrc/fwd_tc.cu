@@ -254,10 +254,10 @@ struct FwdTcFinaliser {
 
 }  // namespace
 
-template <bool COUNT>
+template <bool COUNT, bool STACKLESS>
 __global__ void __launch_bounds__(192, kMinBlocks)
     k_forward_tc(const float4* __restrict__ s_sorted, int64_t S, const uint2* __restrict__ bdesc,
-                 const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes,
+                 const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes, int64_t n_internal,
                  const GaussRec* __restrict__ recs, float* __restrict__ out_cells, float* __restrict__ out_weights,
                  int* status, unsigned long long* stats) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -330,8 +330,8 @@ __global__ void __launch_bounds__(192, kMinBlocks)
             sg.flush();  // the pending batch belongs to the previous group
             sg.g = g;
             const float4 glo = bboxes[2 * (blk * kBlockGroups + g)], ghi = bboxes[2 * (blk * kBlockGroups + g) + 1];
-            st |= warp_traverse(nodes, make_float3(glo.x, glo.y, glo.z), make_float3(ghi.x, ghi.y, ghi.z), sm.stack,
-                                sm.cand, sg, tc);
+            st |= warp_traverse_sel<STACKLESS>(nodes, n_internal, make_float3(glo.x, glo.y, glo.z),
+                                               make_float3(ghi.x, ghi.y, ghi.z), sm.stack, sm.cand, sg, tc);
         }
         sg.flush();
         if (st && lane == 0) atomicOr(status, st);
@@ -466,21 +466,23 @@ __global__ void __launch_bounds__(192, kMinBlocks)
     if (w == 0) tmem_dealloc(tmem, kStages * kBatch);
 }
 
-template <bool COUNT>
+template <bool COUNT, bool STACKLESS>
 static cudaError_t launch_fwd_tc_impl(const CtaArgs& a, cudaStream_t st) {
     const size_t smem = sizeof(FwdTcSmem) + 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_forward_tc<COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_forward_tc<COUNT, STACKLESS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned nb = (unsigned)((a.S + kBlockRows - 1) / kBlockRows);
-    k_forward_tc<COUNT><<<nb, 192, smem, st>>>(a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.recs, a.out_cells,
-                                               a.out_weights, a.status, a.stats);
+    k_forward_tc<COUNT, STACKLESS><<<nb, 192, smem, st>>>(a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.n_internal,
+                                                          a.recs, a.out_cells, a.out_weights, a.status, a.stats);
     gvc::note_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_forward_tc(const CtaArgs& a, cudaStream_t st) {
     if (a.S <= 0) return cudaSuccess;
-    return a.count ? launch_fwd_tc_impl<true>(a, st) : launch_fwd_tc_impl<false>(a, st);
+    if (a.stackless) return a.count ? launch_fwd_tc_impl<true, true>(a, st) : launch_fwd_tc_impl<false, true>(a, st);
+    return a.count ? launch_fwd_tc_impl<true, false>(a, st) : launch_fwd_tc_impl<false, false>(a, st);
 }
 
 }  // namespace gvc

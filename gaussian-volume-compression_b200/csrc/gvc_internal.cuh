@@ -39,8 +39,10 @@ struct __align__(16) GaussRec {
 
 // LBVH internal node with both children's boxes: 64 bytes.
 //   a = (L.lo.xyz, left child bits), b = (L.hi.xyz, right child bits),
-//   c = (R.lo.xyz, 0),               d = (R.hi.xyz, 0)
-// Child encoding: internal node k >= 0; leaf i stored as (i | 0x80000000).
+//   c = (R.lo.xyz, escape edge),     d = (R.hi.xyz, right child bits)
+// Child encoding: internal node k >= 0; leaf i stored as (i | 0x80000000).  The escape
+// edge (2p + s: child s of node p, 0xffffffff for none) is the edge that follows this
+// node's subtree in pre-order; the stackless traversal (traverse.cuh) walks by it.
 struct __align__(16) BvhNode {
     float4 a, b, c, d;
 };
@@ -95,6 +97,7 @@ struct gvc_ctx {
     int cov_grad_mode = 0;
     int bwd_mode = 0;
     int eval_path = 0;
+    int traversal = 0;      // 0 = node stack, 1 = stackless (GVC_OPT_TRAVERSAL)
     int count_pairs = 0;
     int time_kernels = 0;   // record CUDA events around the evaluation kernels
     double fwd_kernel_ms = 0.0, bwd_kernel_ms = 0.0;

@@ -467,8 +467,14 @@ __global__ void __launch_bounds__(256) k_refit(int n, const int32_t* __restrict_
     }
 }
 
+// Packs node k with both children's boxes, and the links of the stackless traversal:
+// c.w = the escape edge of node k (the edge that follows k's subtree in pre-order, edge
+// code 2p + s for child s of node p): (p, 1) for the nearest ancestor-or-self of k that
+// is the left child of p, 0xffffffff when k lies on the root's right spine; d.w = the
+// right child again.
 __global__ void __launch_bounds__(256) k_pack_nodes(int n, const int32_t* __restrict__ left,
                                                     const int32_t* __restrict__ right,
+                                                    const int32_t* __restrict__ parent,
                                                     const float4* __restrict__ leaf_boxes,
                                                     const float4* __restrict__ node_boxes, BvhNode* __restrict__ nodes) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -479,8 +485,8 @@ __global__ void __launch_bounds__(256) k_pack_nodes(int n, const int32_t* __rest
             BvhNode nd;
             nd.a = make_float4(lo.x, lo.y, lo.z, __uint_as_float(0u | kLeafBit));
             nd.b = make_float4(hi.x, hi.y, hi.z, __uint_as_float(0u | kLeafBit));
-            nd.c = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
-            nd.d = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+            nd.c = make_float4(INFINITY, INFINITY, INFINITY, __uint_as_float(0xffffffffu));
+            nd.d = make_float4(-INFINITY, -INFINITY, -INFINITY, __uint_as_float(0u | kLeafBit));
             nodes[0] = nd;
         }
         return;
@@ -493,8 +499,15 @@ __global__ void __launch_bounds__(256) k_pack_nodes(int n, const int32_t* __rest
     BvhNode nd;
     nd.a = make_float4(alo.x, alo.y, alo.z, __int_as_float(l));
     nd.b = make_float4(ahi.x, ahi.y, ahi.z, __int_as_float(r));
-    nd.c = make_float4(blo.x, blo.y, blo.z, 0.f);
-    nd.d = make_float4(bhi.x, bhi.y, bhi.z, 0.f);
+    // escape edge: climb while the node is its parent's right child (at most the depth)
+    int32_t x = k, p = parent[k];
+    for (int depth = 0; p >= 0 && right[p] == x && depth < n; depth++) {
+        x = p;
+        p = parent[p];
+    }
+    const uint32_t esc = p < 0 ? 0xffffffffu : 2u * (uint32_t)p + 1u;
+    nd.c = make_float4(blo.x, blo.y, blo.z, __uint_as_float(esc));
+    nd.d = make_float4(bhi.x, bhi.y, bhi.z, __int_as_float(r));
     nodes[k] = nd;
 }
 
@@ -529,7 +542,7 @@ cudaError_t lbvh_hierarchy(Lbvh& L, int64_t n, const uint32_t* sorted_keys, cons
                                                     L.node_boxes.as<float4>(), L.flags.as<uint32_t>()); gvc::note_launch();
     }
     k_pack_nodes<<<blocks_for(ni, 256), 256, 0, st>>>((int)n, L.left.as<int32_t>(), L.right.as<int32_t>(),
-                                                     sorted_leaf_boxes, L.node_boxes.as<float4>(),
+                                                     L.parent.as<int32_t>(), sorted_leaf_boxes, L.node_boxes.as<float4>(),
                                                      L.nodes.as<BvhNode>()); gvc::note_launch();
     return cudaGetLastError();
 }

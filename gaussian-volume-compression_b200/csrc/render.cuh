@@ -36,7 +36,9 @@ struct BwdArgs {
     const uint32_t* gdesc;     // [n_tiles]
     int64_t n_tiles;
     const BvhNode* tnodes;  // sample-group LBVH
-    const BvhNode* gnodes;  // Gaussian LBVH (atomic mode)
+    const BvhNode* gnodes;  // Gaussian LBVH (atomic and tensor-core modes)
+    int64_t g_internal;     // its internal nodes
+    bool stackless;         // tensor-core mode: traverse by escape edges (warp_traverse_stackless)
     const GaussRec* recs;   // LBVH order (atomic mode)
     float* gacc;            // [P][16] caller order
     int* status;
@@ -53,6 +55,8 @@ struct CtaArgs {
     const uint2* bdesc;    // [n_blocks] block-group descriptors
     const float4* bboxes;  // [n_blocks * 8] block-group boxes (lo, hi)
     const BvhNode* gnodes;
+    int64_t n_internal;    // internal nodes of gnodes
+    bool stackless;        // traverse by escape edges (warp_traverse_stackless)
     const GaussRec* recs;
     float* out_cells;
     float* out_weights;

@@ -17,7 +17,7 @@ STATUS_NAMES = {
     0: "GVC_OK", 1: "GVC_ERR_ARG", 2: "GVC_ERR_CUDA", 3: "GVC_ERR_CAPACITY",
     4: "GVC_ERR_TRAVERSAL", 5: "GVC_ERR_UNSUPPORTED", 6: "GVC_ERR_STATE",
 }
-OPT_COV_GRAD, OPT_BWD_MODE, OPT_EVAL_PATH, OPT_COUNT_PAIRS, OPT_TIME_KERNELS = 1, 2, 3, 4, 5
+OPT_COV_GRAD, OPT_BWD_MODE, OPT_EVAL_PATH, OPT_COUNT_PAIRS, OPT_TIME_KERNELS, OPT_TRAVERSAL = 1, 2, 3, 4, 5, 6
 DTYPE_CODES = {"float64": 0, "float32": 1, "uint16": 2, "uint8": 3}
 
 _vp = ctypes.c_void_p
@@ -45,6 +45,7 @@ _SIGNATURES = {
     "gvc_knn3_mean_dist2": [_vp, _i64, _vp, _vp, _vp],
     "gvc_training_samples": [_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, ctypes.c_uint64, _vp, _vp, _vp],
     "gvc_debug_lbvh": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "gvc_debug_lbvh_escape": [_vp, _vp, _vp],
     "gvc_debug_preprocess": [_vp, _i64, _vp, _vp, _vp, _vp, _f32, _vp, _vp, _vp],
     "gvc_debug_sample_order": [_vp, _vp, _vp, _vp],
     "gvc_debug_tc_gemm": [_vp, _vp, _vp, _int, _vp, _vp],

@@ -57,8 +57,15 @@ typedef enum {
                                    tcgen05 BF16 3-way split MMA into TMEM,
                                2 = FP32 exponent, one warp per 32-sample tile               */
     GVC_OPT_COUNT_PAIRS = 4,/* 1 = record per-call pair counts (gvc_get_stats)            */
-    GVC_OPT_TIME_KERNELS = 5 /* 1 = time the evaluation kernels with CUDA events on the
+    GVC_OPT_TIME_KERNELS = 5,/* 1 = time the evaluation kernels with CUDA events on the
                                 caller's stream (gvc_get_stats)                          */
+    GVC_OPT_TRAVERSAL = 6   /* Gaussian-LBVH traversal of the block-group forwards (eval
+                               paths 0 and 1) and of the tensor-core backward (same
+                               candidates, same results up to summation order):
+                               0 = warp-cooperative with a shared-memory node stack (default),
+                               1 = stackless: level-synchronous descent while a level's
+                                   overlapping nodes fit the warp, then one subtree per lane
+                                   walked by escape edges stored in the nodes              */
 } gvc_option;
 
 typedef struct {
@@ -204,6 +211,12 @@ int gvc_sample_tets_static(int64_t npts, const float* pts, int64_t C, const int3
    builder is cuBQL::cuda::radixBuilder, rasterizer_impl.cu:82). */
 int gvc_debug_lbvh(gvc_ctx* ctx, int64_t n, const float* boxes, uint32_t* keys_sorted, int32_t* perm,
                    int32_t* left, int32_t* right, float* node_boxes, void* stream);
+
+/* Test hook: the escape edges of the stackless traversal in the tree of the last
+   gvc_debug_lbvh call: escape [max(n-1, 1)] int32 (device), per internal node the edge
+   2p + s (child s of node p) that follows its subtree in pre-order, -1 for none.  No
+   counterpart in the reference. */
+int gvc_debug_lbvh_escape(gvc_ctx* ctx, int32_t* escape, void* stream);
 
 /* Test hook: the forward's preprocess (FORWARD::preprocess, forward.cu:10-114) alone:
    conics [6P] and AABBs [P,6] in the caller's order. */

@@ -36,7 +36,8 @@ def test_reference_arm_line():
     # the same config object as our arm prints for the same arguments
     sys.path.insert(0, ROOT)
     import bench
-    ns = type("A", (), {"eval_path": "plain", "bwd_mode": "tensor_core", "use_gaussian_bvh": False})()
+    ns = type("A", (), {"eval_path": "plain", "bwd_mode": "tensor_core", "use_gaussian_bvh": False,
+                       "traversal": "stack"})()
     P, S, desc = bench.CONFIGS["tiny"]
     assert line["config"] == bench.config_dict(ns, desc, P, S, 1)
 
