@@ -136,10 +136,12 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     fence_proxy_async_smem();
     if (t < kBRows) {
         const int64_t row = blk * kBRows + t;
-        float4 p = make_float4(NAN, NAN, NAN, 0.f);
+        // rows past the end at +inf (outside every box); + 0 turns -0 into +0, which the
+        // sign-bit box test below needs
+        float4 p = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
         if (row < n_slots) {
             const float4 q = s_grad[row];
-            p = make_float4(q.x, q.y, q.z, s_ok[row] ? 1.f : 0.f);
+            p = make_float4(q.x + 0.0f, q.y + 0.0f, q.z + 0.0f, s_ok[row] ? 1.f : 0.f);
         }
         sm.rx[t] = p.x;
         sm.ry[t] = p.y;
@@ -288,6 +290,12 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                          nmz = make_float2(-g.mz, -g.mz);
             const float2 Q0 = make_float2(g.q0, g.q0), Q1 = make_float2(g.q1, g.q1), Q2 = make_float2(g.q2, g.q2),
                          Q3 = make_float2(g.q3, g.q3), Q4 = make_float2(g.q4, g.q4), Q5 = make_float2(g.q5, g.q5);
+            // box and window as signs of differences: lo <= x <=> x - lo has its sign bit clear,
+            // exact for finite values once neither x nor hi is -0 (rows and hi get + 0)
+            const float2 NLX = make_float2(-g.lx, -g.lx), NLY = make_float2(-g.ly, -g.ly),
+                         NLZ = make_float2(-g.lz, -g.lz);
+            const float2 HX = make_float2(g.hx + 0.0f, g.hx + 0.0f), HY = make_float2(g.hy + 0.0f, g.hy + 0.0f),
+                         HZ = make_float2(g.hz + 0.0f, g.hz + 0.0f);
             bool okc = true;
             for (int q = q0; q <= q1; q++, j++) {
                 const int b = (int)(j & 1u);
@@ -312,18 +320,25 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                     const float2 X = *reinterpret_cast<const float2*>(&sm.rx[r]);
                     const float2 Y = *reinterpret_cast<const float2*>(&sm.ry[r]);
                     const float2 Z = *reinterpret_cast<const float2*>(&sm.rz[r]);
-                    const bool in0 = ((rmask >> k) & 1u) && g.lx <= X.x && X.x <= g.hx && g.ly <= Y.x && Y.x <= g.hy &&
-                                     g.lz <= Z.x && Z.x <= g.hz;
-                    const bool in1 = ((rmask >> (k + 1)) & 1u) && g.lx <= X.y && X.y <= g.hx && g.ly <= Y.y &&
-                                     Y.y <= g.hy && g.lz <= Z.y && Z.y <= g.hz;
+                    // rows of the chunk outside the group need no mask: their Psi rows are zero
+                    const float2 M1 = make_float2(-1.0f, -1.0f);
+                    const float2 lx2 = __fadd2_rn(X, NLX), ly2 = __fadd2_rn(Y, NLY), lz2 = __fadd2_rn(Z, NLZ);
+                    const float2 hx2 = __ffma2_rn(X, M1, HX), hy2 = __ffma2_rn(Y, M1, HY), hz2 = __ffma2_rn(Z, M1, HZ);
+                    const uint32_t b0 = __float_as_uint(lx2.x) | __float_as_uint(ly2.x) | __float_as_uint(lz2.x) |
+                                        __float_as_uint(hx2.x) | __float_as_uint(hy2.x) | __float_as_uint(hz2.x);
+                    const uint32_t b1 = __float_as_uint(lx2.y) | __float_as_uint(ly2.y) | __float_as_uint(lz2.y) |
+                                        __float_as_uint(hx2.y) | __float_as_uint(hy2.y) | __float_as_uint(hz2.y);
                     const float2 dX = __fadd2_rn(X, nmx), dY = __fadd2_rn(Y, nmy), dZ = __fadd2_rn(Z, nmz);
                     // p2 = dx (q0 dx + q1 dy + q2 dz) + dy (q3 dy + q4 dz) + dz (q5 dz)
                     float2 a = __ffma2_rn(Q0, dX, __ffma2_rn(Q1, dY, __fmul2_rn(Q2, dZ)));
                     a = __fmul2_rn(dX, a);
                     a = __ffma2_rn(dY, __ffma2_rn(Q3, dY, __fmul2_rn(Q4, dZ)), a);
                     const float2 P2 = __ffma2_rn(dZ, __fmul2_rn(Q5, dZ), a);
-                    const bool c0 = in0 && P2.x >= kLog2Floor && P2.x <= 0.0f;
-                    const bool c1 = in1 && P2.y >= kLog2Floor && P2.y <= 0.0f;
+                    // window kLog2Floor <= p2 <= 0: p2 - floor and 0 - p2 (as -p2 + 0: +0 for p2 = -0)
+                    const float2 wl = __fadd2_rn(P2, make_float2(-kLog2Floor, -kLog2Floor));
+                    const float2 wh = __ffma2_rn(P2, M1, make_float2(0.0f, 0.0f));
+                    const bool c0 = (int)(b0 | __float_as_uint(wl.x) | __float_as_uint(wh.x)) >= 0;
+                    const bool c1 = (int)(b1 | __float_as_uint(wl.y) | __float_as_uint(wh.y)) >= 0;
                     const float e0 = c0 ? ex2_approx(P2.x) : 0.f, e1 = c1 ? ex2_approx(P2.y) : 0.f;
                     // E in two BF16 parts (~16 bits: e to 2^-16 relative); Psi keeps three
                     const __nv_bfloat162 H = __floats2bfloat162_rn(e0, e1);
@@ -331,8 +346,9 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                     hw[k >> 1] = *reinterpret_cast<const uint32_t*>(&H);
                     mw[k >> 1] = *reinterpret_cast<const uint32_t*>(&M);
                     if (COUNT) {
-                        ncand += (in0 ? 1 : 0) + (in1 ? 1 : 0);
-                        ncontrib += ((c0 && sm.rok[r]) ? 1 : 0) + ((c1 && sm.rok[r + 1]) ? 1 : 0);
+                        const bool g0 = (rmask >> k) & 1u, g1 = (rmask >> (k + 1)) & 1u;
+                        ncand += ((g0 && (int)b0 >= 0) ? 1 : 0) + ((g1 && (int)b1 >= 0) ? 1 : 0);
+                        ncontrib += ((g0 && c0 && sm.rok[r]) ? 1 : 0) + ((g1 && c1 && sm.rok[r + 1]) ? 1 : 0);
                         nlane += 64;
                     }
                 }
