@@ -203,6 +203,13 @@ def set_traversal(kind, device=None):
     set_option(_n.OPT_TRAVERSAL, {"stack": 0, "stackless": 1}[kind], device)
 
 
+def set_candidate_log(on, device=None):
+    """With the tensor-core backward selected, the forward records each block's candidate
+    Gaussians and the backward reads them back instead of walking the tree again (on by
+    default; off: the backward walks the tree on its own, finer block groups)."""
+    set_option(_n.OPT_CAND_LOG, 1 if on else 0, device)
+
+
 def set_count_pairs(on, device=None):
     set_option(_n.OPT_COUNT_PAIRS, 1 if on else 0, device)
 

@@ -110,7 +110,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     const BvhNode* __restrict__ gnodes, int64_t n_internal, const GaussRec* __restrict__ recs,
     const int32_t* __restrict__ gperm,
     const float4* __restrict__ s_grad, const float* __restrict__ s_gyz, const uint8_t* __restrict__ s_ok,
-    float* __restrict__ gacc, int* status, unsigned long long* stats) {
+    const int32_t* __restrict__ clog, const int32_t* __restrict__ cend, float* __restrict__ gacc, int* status,
+    unsigned long long* stats) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     BwdSmem& sm = *reinterpret_cast<BwdSmem*>(smem_raw);
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
@@ -163,11 +164,39 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
         BwdProducer pr{sm, status, 0u, 0, 0, false};
         TravCount tc;
         int st = 0;
+        // with the forward's candidate log (the groups are then the forward's), the block's
+        // candidates are read back instead of walking the tree: 128 ids per round trip
+        const int gend = (clog && lane < ng) ? cend[blk * kBGroups + lane] : -1;
+        const bool from_log = clog && __shfl_sync(0xffffffffu, gend, 0) >= 0;
+        const int32_t* blog = clog ? clog + blk * kCandLogPerBlock : nullptr;
         for (int g = 0; g < ng && !pr.failed; g++) {
             pr.g = g;
-            const float4 glo = bboxes[2 * (blk * kBGroups + g)], ghi = bboxes[2 * (blk * kBGroups + g) + 1];
-            st |= warp_traverse_sel<STACKLESS>(gnodes, n_internal, make_float3(glo.x, glo.y, glo.z),
-                                               make_float3(ghi.x, ghi.y, ghi.z), sm.stack, sm.tcand, pr, tc);
+            if (from_log) {
+                const int a = g > 0 ? __shfl_sync(0xffffffffu, gend, g - 1) : 0;
+                const int b = __shfl_sync(0xffffffffu, gend, g);
+                for (int off = a; off < b && !pr.failed; off += 128) {
+                    int ids[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int i = off + 32 * u + lane;
+                        ids[u] = i < b ? __ldg(blog + i) : 0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int nb = min(32, b - (off + 32 * u));  // warp-uniform
+                        if (nb > 0) {
+                            sm.tcand[lane] = ids[u];
+                            __syncwarp();
+                            pr(sm.tcand, nb);
+                            tc.leaves += nb;
+                        }
+                    }
+                }
+            } else {
+                const float4 glo = bboxes[2 * (blk * kBGroups + g)], ghi = bboxes[2 * (blk * kBGroups + g) + 1];
+                st |= warp_traverse_sel<STACKLESS>(gnodes, n_internal, make_float3(glo.x, glo.y, glo.z),
+                                                   make_float3(ghi.x, ghi.y, ghi.z), sm.stack, sm.tcand, pr, tc);
+            }
             if (pr.fill > 0 && !pr.failed) pr.publish(pr.fill);
         }
         if (lane == 0) {
@@ -435,7 +464,7 @@ static cudaError_t launch_bwd_cta_impl(const BwdArgs& a, int64_t n_blocks, const
     if (e != cudaSuccess) return e;
     k_backward_cta<COUNT, STACKLESS><<<(unsigned)n_blocks, kBRows + 64, smem, st>>>(
         a.n_tiles * kTile, bdesc, bboxes, a.gnodes, a.g_internal, a.recs, a.gperm, a.s_grad, a.s_gyz, a.s_ok,
-        a.gacc, a.status, a.stats);
+        a.clog, a.cend, a.gacc, a.status, a.stats);
     gvc::note_launch();
     return cudaGetLastError();
 }

@@ -194,7 +194,8 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
         for (DevBuf* b : bufs) b->release();
     }
     DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->blk_desc_b, &c->blk_boxes_b, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
-                      &c->m_out_sorted, &c->knn_boxes, &c->ts_points, &c->ts_words, &c->ts_gt64, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out};
+                      &c->m_out_sorted, &c->knn_boxes, &c->ts_points, &c->ts_words, &c->ts_gt64, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out,
+                      &c->clog, &c->cend};
     for (DevBuf* b : bufs) b->release();
     if (c->d_status) cudaFree(c->d_status);
     if (c->d_stats) cudaFree(c->d_stats);
@@ -224,6 +225,9 @@ int gvc_set_option(gvc_ctx* ctx, int option, int value) {
             return GVC_OK;
         case GVC_OPT_COUNT_PAIRS:
             ctx->count_pairs = value ? 1 : 0;
+            return GVC_OK;
+        case GVC_OPT_CAND_LOG:
+            ctx->cand_log = value ? 1 : 0;
             return GVC_OK;
         case GVC_OPT_TRAVERSAL:
             if (value < 0 || value > 1) return fail(ctx, GVC_ERR_ARG, "traversal must be 0 or 1");
@@ -312,6 +316,7 @@ int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int 
     ctx->n_tiles = (S + kTile - 1) / kTile;
     ctx->samples_ready = false;
     ctx->blk_b_ready = false;
+    ctx->clog_ready = false;
     ctx->tiles_ready = false;        // the sample-group LBVH is built by its first user
     ctx->tile_groups_ready = false;  // so are the lane groups of the 32-sample tiles
     if (S > 0) {
@@ -367,6 +372,7 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
     if (P == 0) {  // rasterize_points.cu:51: outputs stay zero
         GVC_CUDA(launch_fill_zero_outputs(S, out_cells, out_weights, st), "zero outputs");
         ctx->gauss_ready = false;
+        ctx->clog_ready = false;
         return GVC_OK;
     }
     if (!means3D || !scales || !rotations || !values || !weights || !conics)
@@ -419,8 +425,19 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
         ca.status = ctx->d_status;
         ca.stats = ctx->d_stats;
         ca.count = ctx->count_pairs != 0;
+        // the candidates are logged for the tensor-core backward when it is the one selected
+        const bool tc_bwd = ctx->bwd_mode == 3 || (ctx->bwd_mode == 0 && ctx->eval_path == 1);
+        if (tc_bwd && ctx->cand_log && ctx->S > 0) {
+            const int64_t n_blocks = (ctx->S + 127) / 128;
+            GVC_CUDA(ctx->clog.ensure(sizeof(int32_t) * kCandLogPerBlock * n_blocks), "alloc candidate log");
+            GVC_CUDA(ctx->cend.ensure(sizeof(int32_t) * 8 * n_blocks), "alloc candidate log ends");
+            ca.clog = ctx->clog.as<int32_t>();
+            ca.cend = ctx->cend.as<int32_t>();
+        }
         GVC_CUDA(launch_forward_cta(ca, ctx->eval_path == 1, st), "forward (CTA)");
+        ctx->clog_ready = ca.clog != nullptr;
     }
+    if (ctx->eval_path == 2) ctx->clog_ready = false;
     timer_end(ctx, st, tk);
     tm.mark();
     ctx->P = P;
@@ -518,18 +535,28 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
             ba.recs = ctx->grec.as<GaussRec>();
             const int tk = timer_begin(ctx, st, 1);
             const int64_t n_blocks = (S + 127) / 128;
-            if (!ctx->blk_b_ready) {
-                GVC_CUDA(ctx->blk_desc_b.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc_b");
-                GVC_CUDA(ctx->blk_boxes_b.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes_b");
-                GVC_CUDA(launch_sample_blocks(S, ctx->s_sorted.as<float4>(), ctx->s_sort.keys.as<uint32_t>(),
-                                              ctx->blk_desc_b.as<uint2>(), ctx->blk_boxes_b.as<float4>(),
-                                              kBlockSplitBackward, st),
-                         "backward block groups");
-                ctx->blk_b_ready = true;
+            // the forward's candidate log, when it belongs to these Gaussians and samples,
+            // replaces the backward's own walk of the tree (on the forward's block groups)
+            const bool use_log = have_order && ctx->clog_ready;
+            const uint2* bdesc = ctx->blk_desc.as<uint2>();
+            const float4* bboxes = ctx->blk_boxes.as<float4>();
+            if (use_log) {
+                ba.clog = ctx->clog.as<int32_t>();
+                ba.cend = ctx->cend.as<int32_t>();
+            } else {
+                if (!ctx->blk_b_ready) {
+                    GVC_CUDA(ctx->blk_desc_b.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc_b");
+                    GVC_CUDA(ctx->blk_boxes_b.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes_b");
+                    GVC_CUDA(launch_sample_blocks(S, ctx->s_sorted.as<float4>(), ctx->s_sort.keys.as<uint32_t>(),
+                                                  ctx->blk_desc_b.as<uint2>(), ctx->blk_boxes_b.as<float4>(),
+                                                  kBlockSplitBackward, st),
+                             "backward block groups");
+                    ctx->blk_b_ready = true;
+                }
+                bdesc = ctx->blk_desc_b.as<uint2>();
+                bboxes = ctx->blk_boxes_b.as<float4>();
             }
-            GVC_CUDA(launch_backward_cta(ba, n_blocks, ctx->blk_desc_b.as<uint2>(), ctx->blk_boxes_b.as<float4>(),
-                                         st),
-                     "backward (tensor core)");
+            GVC_CUDA(launch_backward_cta(ba, n_blocks, bdesc, bboxes, st), "backward (tensor core)");
             timer_end(ctx, st, tk);
         } else if (atomic_mode) {
             if (!have_order) GVC_CUDA(lbvh_build_boxes(ctx->gbvh, P, boxes, st), "Gaussian LBVH");

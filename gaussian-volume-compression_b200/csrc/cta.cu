@@ -271,6 +271,7 @@ struct Producer {
     int pend_stage, pend_nb;
     int g;
     bool failed;
+    CandLog log;  // the block's candidates for the tensor-core backward (ids null: off)
 
     // waits until the consumers have released the previous use of the stage of batch n
     __device__ __forceinline__ bool acquire_batch(uint32_t n) {
@@ -317,6 +318,7 @@ struct Producer {
 
     __device__ __forceinline__ void operator()(const int* c, int nb) {
         const int lane = threadIdx.x & 31;
+        log.append(c, nb);
         if (failed || !acquire_batch(total)) {
             failed = true;
             __syncwarp();
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(kConsumerWarps * 32 + 32, kCtaMinBlocks)
     k_forward_cta(const float4* __restrict__ s_sorted, int64_t S, const uint2* __restrict__ bdesc,
                   const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes, int64_t n_internal,
                   const GaussRec* __restrict__ recs, float* __restrict__ out_cells, float* __restrict__ out_weights,
-                  int* status, unsigned long long* stats) {
+                  int32_t* __restrict__ clog, int32_t* __restrict__ cend, int* status, unsigned long long* stats) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smem_raw);
     constexpr int RPT = kRowsPerThread;
@@ -367,6 +369,7 @@ __global__ void __launch_bounds__(kConsumerWarps * 32 + 32, kCtaMinBlocks)
     if (w == kConsumerWarps) {
         // ---------------- producer ----------------
         Producer pr{sm, recs, status, 0u, false, 0, 0, 0, false};
+        if (clog) pr.log.ids = clog + blk * kCandLogPerBlock;
         TravCount tc;
         int st = 0;
         for (int g = 0; g < ng && !pr.failed; g++) {
@@ -403,7 +406,10 @@ __global__ void __launch_bounds__(kConsumerWarps * 32 + 32, kCtaMinBlocks)
             __syncwarp();
             st |= warp_traverse_sel<STACKLESS>(nodes, n_internal, make_float3(glo.x, glo.y, glo.z),
                                                make_float3(ghi.x, ghi.y, ghi.z), sm.stack, sm.cand, pr, tc);
+            pr.log.end_group(g);
         }
+        if (pr.failed || st) pr.log.over = true;
+        if (clog) pr.log.finish(cend + blk * kBlockGroups, ng);
         pr.flush();
         if (st && lane == 0) atomicOr(status, st);
         // end marker
@@ -545,8 +551,8 @@ static cudaError_t launch_cta_impl(const CtaArgs& a, cudaStream_t st) {
         cudaFuncSetAttribute(k_forward_cta<COUNT, STACKLESS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_forward_cta<COUNT, STACKLESS><<<nblk128(a.S), kConsumerWarps * 32 + 32, smem, st>>>(
-        a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.n_internal, a.recs, a.out_cells, a.out_weights, a.status,
-        a.stats);
+        a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.n_internal, a.recs, a.out_cells, a.out_weights, a.clog,
+        a.cend, a.status, a.stats);
     gvc::note_launch();
     return cudaGetLastError();
 }

@@ -105,6 +105,7 @@ struct FwdTcStager {
     int pend_stage = 0, pend_nb = 0;
     int g = 0;
     bool failed = false;
+    CandLog log;  // the block's candidates for the tensor-core backward (ids null: off)
 
     __device__ __forceinline__ bool acquire(uint32_t n) {
         const uint32_t k = n / kStages;
@@ -132,6 +133,7 @@ struct FwdTcStager {
 
     __device__ __forceinline__ void operator()(const int* c, int nb) {
         const int lane = threadIdx.x & 31;
+        log.append(c, nb);
         if (failed || !acquire(total)) {
             failed = true;
             __syncwarp();
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(192, kMinBlocks)
     k_forward_tc(const float4* __restrict__ s_sorted, int64_t S, const uint2* __restrict__ bdesc,
                  const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes, int64_t n_internal,
                  const GaussRec* __restrict__ recs, float* __restrict__ out_cells, float* __restrict__ out_weights,
-                 int* status, unsigned long long* stats) {
+                 int32_t* __restrict__ clog, int32_t* __restrict__ cend, int* status, unsigned long long* stats) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     FwdTcSmem& sm = *reinterpret_cast<FwdTcSmem*>(
         smem_raw + ((1024 - (static_cast<uint32_t>(__cvta_generic_to_shared(smem_raw)) & 1023)) & 1023));
@@ -324,6 +326,7 @@ __global__ void __launch_bounds__(192, kMinBlocks)
     if (w == 4) {
         // ---------------- stager: traversal and record copies ----------------
         FwdTcStager sg{sm, recs, status};
+        if (clog) sg.log.ids = clog + blk * kCandLogPerBlock;
         TravCount tc;
         int st = 0;
         for (int g = 0; g < ng && !sg.failed; g++) {
@@ -332,7 +335,10 @@ __global__ void __launch_bounds__(192, kMinBlocks)
             const float4 glo = bboxes[2 * (blk * kBlockGroups + g)], ghi = bboxes[2 * (blk * kBlockGroups + g) + 1];
             st |= warp_traverse_sel<STACKLESS>(nodes, n_internal, make_float3(glo.x, glo.y, glo.z),
                                                make_float3(ghi.x, ghi.y, ghi.z), sm.stack, sm.cand, sg, tc);
+            sg.log.end_group(g);
         }
+        if (sg.failed || st) sg.log.over = true;
+        if (clog) sg.log.finish(cend + blk * kBlockGroups, ng);
         sg.flush();
         if (st && lane == 0) atomicOr(status, st);
         if (!sg.failed && sg.acquire(sg.total)) {
@@ -474,7 +480,8 @@ static cudaError_t launch_fwd_tc_impl(const CtaArgs& a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     const unsigned nb = (unsigned)((a.S + kBlockRows - 1) / kBlockRows);
     k_forward_tc<COUNT, STACKLESS><<<nb, 192, smem, st>>>(a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.n_internal,
-                                                          a.recs, a.out_cells, a.out_weights, a.status, a.stats);
+                                                          a.recs, a.out_cells, a.out_weights, a.clog, a.cend,
+                                                          a.status, a.stats);
     gvc::note_launch();
     return cudaGetLastError();
 }

@@ -98,6 +98,7 @@ struct gvc_ctx {
     int bwd_mode = 0;
     int eval_path = 0;
     int traversal = 0;      // 0 = node stack, 1 = stackless (GVC_OPT_TRAVERSAL)
+    int cand_log = 1;       // GVC_OPT_CAND_LOG
     int count_pairs = 0;
     int time_kernels = 0;   // record CUDA events around the evaluation kernels
     double fwd_kernel_ms = 0.0, bwd_kernel_ms = 0.0;
@@ -111,6 +112,9 @@ struct gvc_ctx {
     int64_t S = 0;
     int64_t n_tiles = 0;
     bool samples_ready = false;
+    // candidate log of the last block-group forward (for the tensor-core backward)
+    gvc::DevBuf clog, cend;
+    bool clog_ready = false;
     gvc::DevBuf s_sorted;   // [n_tiles*32] float4 (x, y, z, bits of caller index or -1)
     gvc::DevBuf tile_boxes; // [n_tiles * kGroups] group boxes, 2 x float4 (empty for unused slots)
     gvc::DevBuf tile_keys;  // [n_tiles * kGroups] uint32 Morton key of each group's first sample

@@ -39,6 +39,8 @@ struct BwdArgs {
     const BvhNode* gnodes;  // Gaussian LBVH (atomic and tensor-core modes)
     int64_t g_internal;     // its internal nodes
     bool stackless;         // tensor-core mode: traverse by escape edges (warp_traverse_stackless)
+    const int32_t* clog;    // tensor-core mode: the forward's candidate log (null: traverse)
+    const int32_t* cend;
     const GaussRec* recs;   // LBVH order (atomic mode)
     float* gacc;            // [P][16] caller order
     int* status;
@@ -47,6 +49,37 @@ struct BwdArgs {
 };
 
 cudaError_t launch_forward(const FwdArgs& a, cudaStream_t st);
+
+// Candidate log of the block-group forwards, read by the tensor-core backward instead of
+// walking the Gaussian LBVH again: the forward's producer appends the candidates of a
+// block's groups in order to the block's kCandLogPerBlock slots, and group g's candidates
+// end at cend[blk * 8 + g]; a block with more candidates than slots gets -1 for every
+// group, and the backward walks the tree for it.
+constexpr int kCandLogPerBlock = 4096;
+
+struct CandLog {
+    int32_t* ids = nullptr;  // this block's slots, or null (no log)
+    int pos = 0;             // candidates appended (warp-uniform)
+    bool over = false;
+    int gend = 0;  // on lane g: end of group g
+
+    __device__ __forceinline__ void append(const int* c, int nb) {
+        if (!ids) return;
+        const int lane = threadIdx.x & 31;
+        if (pos + nb <= kCandLogPerBlock) {
+            if (lane < nb) ids[pos + lane] = c[lane];
+        } else {
+            over = true;
+        }
+        pos += nb;
+    }
+    __device__ __forceinline__ void end_group(int g) {
+        if ((threadIdx.x & 31) == g) gend = pos;
+    }
+    __device__ __forceinline__ void finish(int32_t* cend_blk, int ng) {
+        if (ids && (int)(threadIdx.x & 31) < ng) cend_blk[threadIdx.x & 31] = over ? -1 : gend;
+    }
+};
 
 // cta.cu: CTA-level forward on 128-sample blocks (tensor-core or SIMT exponent)
 struct CtaArgs {
@@ -57,6 +90,8 @@ struct CtaArgs {
     const BvhNode* gnodes;
     int64_t n_internal;    // internal nodes of gnodes
     bool stackless;        // traverse by escape edges (warp_traverse_stackless)
+    int32_t* clog;         // candidate log [n_blocks * kCandLogPerBlock], or null
+    int32_t* cend;         // group ends of the log [n_blocks * 8]
     const GaussRec* recs;
     float* out_cells;
     float* out_weights;

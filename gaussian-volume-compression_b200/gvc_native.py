@@ -18,6 +18,7 @@ STATUS_NAMES = {
     4: "GVC_ERR_TRAVERSAL", 5: "GVC_ERR_UNSUPPORTED", 6: "GVC_ERR_STATE",
 }
 OPT_COV_GRAD, OPT_BWD_MODE, OPT_EVAL_PATH, OPT_COUNT_PAIRS, OPT_TIME_KERNELS, OPT_TRAVERSAL = 1, 2, 3, 4, 5, 6
+OPT_CAND_LOG = 7
 DTYPE_CODES = {"float64": 0, "float32": 1, "uint16": 2, "uint8": 3}
 
 _vp = ctypes.c_void_p

@@ -59,13 +59,19 @@ typedef enum {
     GVC_OPT_COUNT_PAIRS = 4,/* 1 = record per-call pair counts (gvc_get_stats)            */
     GVC_OPT_TIME_KERNELS = 5,/* 1 = time the evaluation kernels with CUDA events on the
                                 caller's stream (gvc_get_stats)                          */
-    GVC_OPT_TRAVERSAL = 6   /* Gaussian-LBVH traversal of the block-group forwards (eval
+    GVC_OPT_TRAVERSAL = 6,  /* Gaussian-LBVH traversal of the block-group forwards (eval
                                paths 0 and 1) and of the tensor-core backward (same
                                candidates, same results up to summation order):
                                0 = warp-cooperative with a shared-memory node stack (default),
                                1 = stackless: level-synchronous descent while a level's
                                    overlapping nodes fit the warp, then one subtree per lane
                                    walked by escape edges stored in the nodes              */
+    GVC_OPT_CAND_LOG = 7    /* 1 (default) = when the tensor-core backward is selected, the
+                               block-group forward records every block's candidate Gaussians
+                               (kCandLogPerBlock = 4096 per 128-sample block, 16 KB) and the
+                               backward reads them back instead of walking the Gaussian LBVH
+                               again (then on the forward's block groups); blocks with more
+                               candidates are walked.  0 = the backward always walks.      */
 } gvc_option;
 
 typedef struct {

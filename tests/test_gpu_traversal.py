@@ -140,5 +140,8 @@ def test_stackless_same_candidates_at_scale(cuda, orc, path):
     v = ok & (oa != -1)
     assert ((np.abs(wb[v] - wa[v]) - 4e-6) / wa[v]).max() <= 2e-5
     assert (np.abs(ob[v] - oa[v]) - 4e-6 / wa[v]).max() <= 2e-5
+    # two runs of the atomic tensor-core backward, each within the oracle tolerance (1e-4 of
+    # max; 5e-4 for the covariance adjoint: scales, rotations), differ by at most twice it
     for k in range(5):
-        assert np.abs(gb[k] - ga[k]).max() <= 5e-4 * np.abs(ga[k]).max()
+        tol = 1e-3 if k in (1, 2) else 2e-4
+        assert np.abs(gb[k] - ga[k]).max() <= tol * np.abs(ga[k]).max(), k
