@@ -110,8 +110,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     const BvhNode* __restrict__ gnodes, int64_t n_internal, const GaussRec* __restrict__ recs,
     const int32_t* __restrict__ gperm,
     const float4* __restrict__ s_grad, const float* __restrict__ s_gyz, const uint8_t* __restrict__ s_ok,
-    const int32_t* __restrict__ clog, const int32_t* __restrict__ cend, float* __restrict__ gacc, int* status,
-    unsigned long long* stats) {
+    const int32_t* __restrict__ clog, const int32_t* __restrict__ cend, const uint2* __restrict__ cdesc,
+    float* __restrict__ gacc, int* status, unsigned long long* stats) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     BwdSmem& sm = *reinterpret_cast<BwdSmem*>(smem_raw);
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
@@ -164,36 +164,55 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
         BwdProducer pr{sm, status, 0u, 0, 0, false};
         TravCount tc;
         int st = 0;
-        // with the forward's candidate log (the groups are then the forward's), the block's
-        // candidates are read back instead of walking the tree: 128 ids per round trip
-        const int gend = (clog && lane < ng) ? cend[blk * kBGroups + lane] : -1;
+        // With the forward's candidate log, the block's candidates are read back instead of
+        // walking the tree.  The log holds the candidates of the forward's groups (cdesc),
+        // each of which contains whole groups of this kernel: a group keeps the candidates
+        // of its enclosing forward group whose boxes overlap its own, 128 per round trip.
+        const uint2 cd = clog ? cdesc[blk] : make_uint2(0u, 0u);
+        const int cng = (int)(cd.y >> 24);
+        const int gend = (clog && lane < cng) ? cend[blk * kBGroups + lane] : -1;
         const bool from_log = clog && __shfl_sync(0xffffffffu, gend, 0) >= 0;
         const int32_t* blog = clog ? clog + blk * kCandLogPerBlock : nullptr;
+        const uint32_t lt = lane_lt_mask();
         for (int g = 0; g < ng && !pr.failed; g++) {
             pr.g = g;
+            const float4 glo = bboxes[2 * (blk * kBGroups + g)], ghi = bboxes[2 * (blk * kBGroups + g) + 1];
             if (from_log) {
-                const int a = g > 0 ? __shfl_sync(0xffffffffu, gend, g - 1) : 0;
-                const int b = __shfl_sync(0xffffffffu, gend, g);
+                const int ra = bgroup_start(bd, g);
+                int G = 0;
+                for (int k = 1; k < cng; k++)
+                    if (ra >= bgroup_start(cd, k)) G = k;
+                const int a = G > 0 ? __shfl_sync(0xffffffffu, gend, G - 1) : 0;
+                const int b = __shfl_sync(0xffffffffu, gend, G);
+                const float3 qlo = make_float3(glo.x, glo.y, glo.z), qhi = make_float3(ghi.x, ghi.y, ghi.z);
                 for (int off = a; off < b && !pr.failed; off += 128) {
                     int ids[4];
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
                         const int i = off + 32 * u + lane;
-                        ids[u] = i < b ? __ldg(blog + i) : 0;
+                        ids[u] = i < b ? __ldg(blog + i) : -1;
+                    }
+                    bool hit[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        hit[u] = false;
+                        if (ids[u] >= 0) {
+                            const float4* rp = reinterpret_cast<const float4*>(recs + ids[u]);
+                            hit[u] = box_overlap(__ldg(rp + 3), __ldg(rp + 4), qlo, qhi);
+                        }
                     }
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
-                        const int nb = min(32, b - (off + 32 * u));  // warp-uniform
-                        if (nb > 0) {
-                            sm.tcand[lane] = ids[u];
+                        const uint32_t m = __ballot_sync(0xffffffffu, hit[u]);  // warp-uniform
+                        if (m) {
+                            if (hit[u]) sm.tcand[__popc(m & lt)] = ids[u];
                             __syncwarp();
-                            pr(sm.tcand, nb);
-                            tc.leaves += nb;
+                            pr(sm.tcand, __popc(m));
+                            tc.leaves += __popc(m);
                         }
                     }
                 }
             } else {
-                const float4 glo = bboxes[2 * (blk * kBGroups + g)], ghi = bboxes[2 * (blk * kBGroups + g) + 1];
                 st |= warp_traverse_sel<STACKLESS>(gnodes, n_internal, make_float3(glo.x, glo.y, glo.z),
                                                    make_float3(ghi.x, ghi.y, ghi.z), sm.stack, sm.tcand, pr, tc);
             }
@@ -464,7 +483,7 @@ static cudaError_t launch_bwd_cta_impl(const BwdArgs& a, int64_t n_blocks, const
     if (e != cudaSuccess) return e;
     k_backward_cta<COUNT, STACKLESS><<<(unsigned)n_blocks, kBRows + 64, smem, st>>>(
         a.n_tiles * kTile, bdesc, bboxes, a.gnodes, a.g_internal, a.recs, a.gperm, a.s_grad, a.s_gyz, a.s_ok,
-        a.clog, a.cend, a.gacc, a.status, a.stats);
+        a.clog, a.cend, a.cdesc, a.gacc, a.status, a.stats);
     gvc::note_launch();
     return cudaGetLastError();
 }

@@ -535,27 +535,24 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
             ba.recs = ctx->grec.as<GaussRec>();
             const int tk = timer_begin(ctx, st, 1);
             const int64_t n_blocks = (S + 127) / 128;
+            if (!ctx->blk_b_ready) {
+                GVC_CUDA(ctx->blk_desc_b.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc_b");
+                GVC_CUDA(ctx->blk_boxes_b.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes_b");
+                GVC_CUDA(launch_sample_blocks(S, ctx->s_sorted.as<float4>(), ctx->s_sort.keys.as<uint32_t>(),
+                                              ctx->blk_desc_b.as<uint2>(), ctx->blk_boxes_b.as<float4>(),
+                                              kBlockSplitBackward, st),
+                         "backward block groups");
+                ctx->blk_b_ready = true;
+            }
             // the forward's candidate log, when it belongs to these Gaussians and samples,
-            // replaces the backward's own walk of the tree (on the forward's block groups)
-            const bool use_log = have_order && ctx->clog_ready;
-            const uint2* bdesc = ctx->blk_desc.as<uint2>();
-            const float4* bboxes = ctx->blk_boxes.as<float4>();
-            if (use_log) {
+            // replaces the backward's own walk of the tree
+            if (have_order && ctx->clog_ready) {
                 ba.clog = ctx->clog.as<int32_t>();
                 ba.cend = ctx->cend.as<int32_t>();
-            } else {
-                if (!ctx->blk_b_ready) {
-                    GVC_CUDA(ctx->blk_desc_b.ensure(sizeof(uint2) * n_blocks), "alloc blk_desc_b");
-                    GVC_CUDA(ctx->blk_boxes_b.ensure(sizeof(float4) * 2 * 8 * n_blocks), "alloc blk_boxes_b");
-                    GVC_CUDA(launch_sample_blocks(S, ctx->s_sorted.as<float4>(), ctx->s_sort.keys.as<uint32_t>(),
-                                                  ctx->blk_desc_b.as<uint2>(), ctx->blk_boxes_b.as<float4>(),
-                                                  kBlockSplitBackward, st),
-                             "backward block groups");
-                    ctx->blk_b_ready = true;
-                }
-                bdesc = ctx->blk_desc_b.as<uint2>();
-                bboxes = ctx->blk_boxes_b.as<float4>();
+                ba.cdesc = ctx->blk_desc.as<uint2>();
             }
+            const uint2* bdesc = ctx->blk_desc_b.as<uint2>();
+            const float4* bboxes = ctx->blk_boxes_b.as<float4>();
             GVC_CUDA(launch_backward_cta(ba, n_blocks, bdesc, bboxes, st), "backward (tensor core)");
             timer_end(ctx, st, tk);
         } else if (atomic_mode) {

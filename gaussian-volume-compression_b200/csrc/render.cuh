@@ -41,6 +41,7 @@ struct BwdArgs {
     bool stackless;         // tensor-core mode: traverse by escape edges (warp_traverse_stackless)
     const int32_t* clog;    // tensor-core mode: the forward's candidate log (null: traverse)
     const int32_t* cend;
+    const uint2* cdesc;     // the forward's block groups (the log's groups)
     const GaussRec* recs;   // LBVH order (atomic mode)
     float* gacc;            // [P][16] caller order
     int* status;

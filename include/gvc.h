@@ -70,8 +70,9 @@ typedef enum {
                                block-group forward records every block's candidate Gaussians
                                (kCandLogPerBlock = 4096 per 128-sample block, 16 KB) and the
                                backward reads them back instead of walking the Gaussian LBVH
-                               again (then on the forward's block groups); blocks with more
-                               candidates are walked.  0 = the backward always walks.      */
+                               again (each of its finer block groups keeps the candidates of
+                               the enclosing forward group whose boxes overlap its own);
+                               blocks with more candidates are walked.  0 = always walk.   */
 } gvc_option;
 
 typedef struct {

@@ -76,8 +76,9 @@ def test_logged_backward_matches_oracle(cuda, orc, small_case, path):
 
 
 def test_logged_equals_walked_at_scale(cuda, orc):
-    """200k clustered Gaussians x 1M samples: the logged backward (forward's block groups)
-    against the backward walking the tree (its own finer groups)."""
+    """200k clustered Gaussians x 1M samples: the logged backward (its groups' candidates
+    filtered from the enclosing forward groups' logs) against the backward walking the
+    tree: the same evaluated rows and contributing pairs, gradients within tolerance."""
     case = orc.mixture_large(seed=4, P=200_000, S=1_000_000)
     S = case[-1].shape[0]
     rng = np.random.default_rng(52)
@@ -91,6 +92,7 @@ def test_logged_equals_walked_at_scale(cuda, orc):
     np.testing.assert_array_equal(wa, wb)
     assert sa["bwd_node_visits"] == 0 and sb["bwd_node_visits"] > 0
     assert sa["bwd_contributing"] == sb["bwd_contributing"]
+    assert sa["bwd_rows"] == sb["bwd_rows"]  # same groups, same candidates per group
     for k in range(5):
         assert np.abs(ga[k] - gb[k]).max() <= 5e-4 * np.abs(gb[k]).max(), k
 
