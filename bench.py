@@ -65,10 +65,10 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # (and of k_backward_gauss with --bwd-mode deterministic); other workloads report null.
 # Tensor-pipe activity (sm__pipe_tc_cycles_active, share of peak) of the tensor-core kernels
 # in their committed --set full captures of the 2M x 4M profiling case (profiles/).
-TENSOR_PIPE_ACTIVE = {"k_backward_cta": 0.324, "k_forward_tc": 0.189}
-MEASURED_TRAFFIC = {("large", "k_backward_cta"): 0.915e9 + 0.134e9,
+TENSOR_PIPE_ACTIVE = {"k_backward_cta": 0.344, "k_forward_tc": 0.189}
+MEASURED_TRAFFIC = {("large", "k_backward_cta"): 1.290e9 + 0.140e9,
                     ("large", "k_backward_gauss"): 1.475e9 + 0.125e9,
-                    ("large", "k_forward_cta"): 1.465e9 + 1.011e9}
+                    ("large", "k_forward_cta"): 1.566e9 + 1.640e9}
 
 
 def parse():
@@ -947,16 +947,19 @@ def run_ours(args):
     grad_runs = {}
     paths_extra = {}
     if not args.profile:
-        # (forward path, backward mode, traversal): FP32 throughout, tensor cores throughout, the
-        # FP32 forward with the tensor-core backward reduction, and that with the stackless
-        # Gaussian-LBVH traversal (timed only)
-        for name, path, bmode, trav in (("plain", "plain", "auto", "stack"),
-                                        ("tensor_core", "tensor_core", "auto", "stack"),
-                                        ("plain_fwd_tc_bwd", "plain", "tensor_core", "stack"),
-                                        ("stackless", "plain", "tensor_core", "stackless")):
+        # (forward path, backward mode, traversal, candidate log): FP32 throughout, tensor cores
+        # throughout, the FP32 forward with the tensor-core backward reduction, and (timed
+        # only) that with the backward walking the tree again instead of reading the forward's
+        # candidate log, and with the stackless Gaussian-LBVH traversal in both kernels
+        for name, path, bmode, trav, clog in (("plain", "plain", "auto", "stack", True),
+                                              ("tensor_core", "tensor_core", "auto", "stack", True),
+                                              ("plain_fwd_tc_bwd", "plain", "tensor_core", "stack", True),
+                                              ("walk", "plain", "tensor_core", "stack", False),
+                                              ("stackless", "plain", "tensor_core", "stackless", False)):
             _C.set_eval_path(path)
             _C.set_backward_mode(bmode)
             _C.set_traversal(trav)
+            _C.set_candidate_log(clog)
             for _ in range(2):
                 step()
             torch.cuda.synchronize()
@@ -969,8 +972,8 @@ def run_ours(args):
             b1.record(stream)
             torch.cuda.synchronize()
             pm = gvc_dist.max_over_ranks(b0.elapsed_time(b1) / args.steps, dev)
-            if name == "stackless":
-                paths_extra["plain_fwd_tc_bwd_stackless_ms_per_step"] = pm
+            if name in ("walk", "stackless"):
+                paths_extra["plain_fwd_tc_bwd_%s_ms_per_step" % name] = pm
                 continue
             # one more step, outputs and gradients kept (untimed)
             _C.build_bvh(d_samples, False, ugb)
@@ -992,6 +995,7 @@ def run_ours(args):
         _C.set_eval_path(args.eval_path)
         _C.set_backward_mode(args.bwd_mode)
         _C.set_traversal(args.traversal)
+        _C.set_candidate_log(True)
         _C.check_status()
 
     cpu = None
@@ -1008,8 +1012,11 @@ def run_ours(args):
                        "paths": {"plain": "FP32 CTA forward + FP32 deterministic Gaussian-owned backward",
                                  "tensor_core": "tcgen05 split-BF16 exponent forward + tcgen05 moment backward",
                                  "plain_fwd_tc_bwd": "FP32 CTA forward + tcgen05 moment backward",
-                                 "plain_fwd_tc_bwd_stackless": "the same with the stackless Gaussian-LBVH "
-                                                               "traversal (escape edges) in both kernels"},
+                                 "plain_fwd_tc_bwd_walk": "the same with the backward walking the Gaussian "
+                                                          "LBVH again instead of reading the forward's "
+                                                          "candidate log",
+                                 "plain_fwd_tc_bwd_stackless": "the same walking in both kernels by the "
+                                                               "stackless traversal (escape edges)"},
                        "fp64_error": fp64}
         tc_vs_plain.update(paths_extra)
 
