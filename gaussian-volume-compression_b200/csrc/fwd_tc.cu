@@ -404,10 +404,14 @@ __global__ void __launch_bounds__(192, kMinBlocks)
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
                     if (!((m16 >> j) & 1u)) continue;
+                    const float p2 = v[j];
+                    const bool win = ing && p2 >= kLog2FloorF && p2 <= kTcZeroTol;
+                    // the window needs no column data: a column none of whose rows in this
+                    // warp is in it contributes nothing here, box test or not
+                    if (!COUNT && !__any_sync(0xffffffffu, win)) continue;
                     const float4 a = sm.colA[s][16 * h + j], b = sm.colB[s][16 * h + j];
                     const bool in = ing && a.x <= x && x <= b.x && a.y <= y && y <= b.y && a.z <= z && z <= b.z;
-                    const float p2 = v[j];
-                    const bool c = in && p2 >= kLog2FloorF && p2 <= kTcZeroTol;
+                    const bool c = in && win;
                     const float e = c ? ex2f(fminf(p2, 0.f)) : 0.f;
                     W = fmaf(a.w, e, W);
                     V = fmaf(b.w, e, V);
