@@ -17,7 +17,9 @@
 // accumulated (the third part of E measured 10 % slower for no gain within tolerance).  Thread t then reads its
 // own row of D, turns the moments about x0 into the moments about its mean (pair.cuh)
 // and adds its eleven gradient terms with FP32 atomics.  An MMA warp issues the products
-// while the consumers compute the next 16-row chunk (two A buffers).
+// while the consumers compute the next 16-row chunk (two A buffers); batches alternate
+// between two TMEM accumulators, so that a batch's read-out waits until the next batch's
+// chunks are issued and its last MMAs drain meanwhile.
 #include "pair.cuh"
 #include "render.cuh"
 #include "tc.cuh"
@@ -41,7 +43,7 @@ struct BwdSmem {
     int2 desc[kBStages];                        // (count or -1 at the end, group)
     int stack[kStackCap];
     int tcand[kCandCap];
-    uint64_t full[kBStages], empty[kBStages], aready[2], afree[2], dready, dfree;
+    uint64_t full[kBStages], empty[kBStages], aready[2], afree[2], dready[2], dfree[2];
     uint32_t tmem_base;
 };
 
@@ -121,14 +123,16 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     if (t == 0) {
         for (int s = 0; s < kBStages; s++) {
             mbar_init(&sm.full[s], 1);
-            mbar_init(&sm.empty[s], 4);
+            mbar_init(&sm.empty[s], 5);  // the four consumer warps and the MMA warp
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&sm.aready[b], 4);
             mbar_init(&sm.afree[b], 1);
         }
-        mbar_init(&sm.dready, 1);
-        mbar_init(&sm.dfree, 4);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&sm.dready[b], 1);
+            mbar_init(&sm.dfree[b], 4);
+        }
         fence_mbar_init();
     }
     // features 20..31 of every Psi tile stay zero
@@ -150,8 +154,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
         sm.rok[t] = p.w != 0.f;
     }
     if (w == 0) {
-        static_assert(tmem_cols_ok(kMom), "TMEM columns must be a power of two >= 32");
-        tmem_alloc(&sm.tmem_base, kMom);
+        static_assert(tmem_cols_ok(2 * kMom), "TMEM columns must be a power of two >= 32");
+        tmem_alloc(&sm.tmem_base, 2 * kMom);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -241,9 +245,11 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 if (!mbar_wait(&sm.full[s], (n / kBStages) & 1u, status)) break;
                 const int2 d = sm.desc[s];
                 if (d.x < 0) break;
+                mbar_arrive(&sm.empty[s]);  // its descriptor is read
                 const int ra = bgroup_start(bd, d.y), rb = bgroup_start(bd, d.y + 1);
                 const int q0 = ra >> 4, q1 = (rb - 1) >> 4;
-                if (n > 0 && !mbar_wait(&sm.dfree, (n - 1) & 1u, status)) break;
+                if (n >= 2 && !mbar_wait(&sm.dfree[n & 1u], ((n >> 1) - 1) & 1u, status)) break;
+                const uint32_t tmem_d = tmem + (n & 1u) * kMom;
                 bool ok = true;
                 for (int q = q0; q <= q1; q++, j++) {
                     const int b = (int)(j & 1u);
@@ -255,15 +261,15 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                     const uint64_t a0 = smem_desc_k16(sm.A[b][0]), a1 = smem_desc_k16(sm.A[b][1]);
                     const uint64_t b0 = smem_desc_k16(sm.B[q][0]), b1 = smem_desc_k16(sm.B[q][1]),
                                    b2 = smem_desc_k16(sm.B[q][2]);
-                    umma_bf16(tmem, a1, b1, idesc, q == q0 ? 0u : 1u);  // mid * mid
-                    umma_bf16(tmem, a0, b2, idesc, 1u);                 // hi * lo
-                    umma_bf16(tmem, a1, b0, idesc, 1u);                 // mid * hi
-                    umma_bf16(tmem, a0, b1, idesc, 1u);                 // hi * mid
-                    umma_bf16(tmem, a0, b0, idesc, 1u);                 // hi * hi
+                    umma_bf16(tmem_d, a1, b1, idesc, q == q0 ? 0u : 1u);  // mid * mid
+                    umma_bf16(tmem_d, a0, b2, idesc, 1u);                 // hi * lo
+                    umma_bf16(tmem_d, a1, b0, idesc, 1u);                 // mid * hi
+                    umma_bf16(tmem_d, a0, b1, idesc, 1u);                 // hi * mid
+                    umma_bf16(tmem_d, a0, b0, idesc, 1u);                 // hi * hi
                     umma_commit(&sm.afree[b]);
                 }
                 if (!ok) break;
-                umma_commit(&sm.dready);
+                umma_commit(&sm.dready[n & 1u]);
             }
         }
         __syncwarp();
@@ -274,6 +280,56 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
         uint32_t j = 0;
         int ncand = 0, ncontrib = 0;
         long long nlane = 0;  // lane slots evaluated (warp-uniform)
+        // The previous batch's read-out is deferred until this batch's chunks are issued,
+        // so that its last MMAs drain meanwhile (two TMEM accumulators, by batch parity).
+        bool pending = false;
+        uint32_t pend_n = 0;
+        int pend_leaf = -1;
+        float px0 = 0.f, py0 = 0.f, pz0 = 0.f;
+        auto drain = [&]() -> bool {
+            const uint32_t pb = pend_n & 1u;
+            pending = false;
+            const bool okd = mbar_wait(&sm.dready[pb], (pend_n >> 1) & 1u, status);
+            if (!__all_sync(0xffffffffu, okd)) return false;
+            tc_fence_after();
+            float v[32];
+            tmem_ld32(tmem + pb * kMom + ((uint32_t)(32 * w) << 16), v);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.dfree[pb]);
+            // a Gaussian without a contributing pair has an all-zero row of D
+            bool anyc = false;
+#pragma unroll
+            for (int k = 0; k < 20; k++) anyc |= v[k] != 0.f;
+            if (anyc && pend_leaf >= 0) {
+                const float4* rp = reinterpret_cast<const float4*>(recs + pend_leaf);
+                const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2);
+                // moments about the group centre -> moments about the mean (d = u - a)
+                const float ax = r0.x - px0, ay = r0.y - py0, az = r0.z - pz0;
+                float S[10];
+#pragma unroll
+                for (int k = 0; k < 10; k++) S[k] = fmaf(r2.z, v[k], v[10 + k]);
+                float m[11];
+                m[0] = v[0];
+                m[1] = S[0];
+                m[2] = S[1] - ax * S[0];
+                m[3] = S[2] - ay * S[0];
+                m[4] = S[3] - az * S[0];
+                m[5] = S[4] - 2.f * ax * S[1] + ax * ax * S[0];
+                m[6] = S[5] - ax * S[2] - ay * S[1] + ax * ay * S[0];
+                m[7] = S[6] - ax * S[3] - az * S[1] + ax * az * S[0];
+                m[8] = S[7] - 2.f * ay * S[2] + ay * ay * S[0];
+                m[9] = S[8] - ay * S[3] - az * S[2] + ay * az * S[0];
+                m[10] = S[9] - 2.f * az * S[3] + az * az * S[0];
+                float tm[11];
+                moments_to_terms_lane(m, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, tm);
+                float4* dst = reinterpret_cast<float4*>(gacc + 16 * (int64_t)gperm[pend_leaf]);
+                atomicAdd(dst, make_float4(tm[0], tm[1], tm[2], tm[3]));
+                atomicAdd(dst + 1, make_float4(tm[4], tm[5], tm[6], tm[7]));
+                atomicAdd(dst + 2, make_float4(tm[8], tm[9], tm[10], 0.f));
+            }
+            return true;
+        };
         for (uint32_t n = 0;; n++) {
             const int s = (int)(n % kBStages);
             const bool okw = mbar_wait(&sm.full[s], (n / kBStages) & 1u, status);
@@ -284,7 +340,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
             const int q0 = ra >> 4, q1 = (rb - 1) >> 4;
             if (d.y != cur_group) {
                 // Psi of this warp's rows (chunks 2w, 2w + 1) for the new group; every MMA of
-                // the previous group has completed (dready of its last batch was awaited).
+                // the previous group has completed once its last batch is drained.
+                if (pending && !drain()) break;
                 cur_group = d.y;
                 const float4 glo = bboxes[2 * (blk * kBGroups + d.y)], ghi = bboxes[2 * (blk * kBGroups + d.y) + 1];
                 x0 = 0.5f * (glo.x + ghi.x);
@@ -333,6 +390,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 blo = __ldg(rp + 3);
                 bhi = __ldg(rp + 4);
             }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.empty[s]);  // the stage's candidates are read
             const GaussB g = gauss_b(r0.x, r0.y, r0.z, r2.z, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, blo, bhi);
             const float2 nmx = make_float2(-g.mx, -g.mx), nmy = make_float2(-g.my, -g.my),
                          nmz = make_float2(-g.mz, -g.mz);
@@ -414,47 +473,15 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 if (lane == 0) mbar_arrive(&sm.aready[b]);
             }
             if (!okc) break;
-            const bool okd = mbar_wait(&sm.dready, n & 1u, status);
-            if (!__all_sync(0xffffffffu, okd)) break;
-            tc_fence_after();
-            float v[32];
-            tmem_ld32(tmem + ((uint32_t)(32 * w) << 16), v);
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(&sm.dfree);
-                mbar_arrive(&sm.empty[s]);
-            }
-            // a Gaussian without a contributing pair has an all-zero row of D
-            bool anyc = false;
-#pragma unroll
-            for (int k = 0; k < 20; k++) anyc |= v[k] != 0.f;
-            if (anyc) {
-                // moments about the group centre -> moments about the mean (d = u - a)
-                const float ax = g.mx - x0, ay = g.my - y0, az = g.mz - z0;
-                float S[10];
-#pragma unroll
-                for (int k = 0; k < 10; k++) S[k] = fmaf(g.v, v[k], v[10 + k]);
-                float m[11];
-                m[0] = v[0];
-                m[1] = S[0];
-                m[2] = S[1] - ax * S[0];
-                m[3] = S[2] - ay * S[0];
-                m[4] = S[3] - az * S[0];
-                m[5] = S[4] - 2.f * ax * S[1] + ax * ax * S[0];
-                m[6] = S[5] - ax * S[2] - ay * S[1] + ax * ay * S[0];
-                m[7] = S[6] - ax * S[3] - az * S[1] + ax * az * S[0];
-                m[8] = S[7] - 2.f * ay * S[2] + ay * ay * S[0];
-                m[9] = S[8] - ay * S[3] - az * S[2] + ay * az * S[0];
-                m[10] = S[9] - 2.f * az * S[3] + az * az * S[0];
-                float tm[11];
-                moments_to_terms_lane(m, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, tm);
-                float4* dst = reinterpret_cast<float4*>(gacc + 16 * (int64_t)gperm[leaf]);
-                atomicAdd(dst, make_float4(tm[0], tm[1], tm[2], tm[3]));
-                atomicAdd(dst + 1, make_float4(tm[4], tm[5], tm[6], tm[7]));
-                atomicAdd(dst + 2, make_float4(tm[8], tm[9], tm[10], 0.f));
-            }
+            if (pending && !drain()) break;
+            pending = true;
+            pend_n = n;
+            pend_leaf = leaf;
+            px0 = x0;
+            py0 = y0;
+            pz0 = z0;
         }
+        if (pending) drain();
         if (COUNT) {
             unsigned long long a = (unsigned long long)ncand, c = (unsigned long long)ncontrib;
             for (int off = 16; off > 0; off >>= 1) {
@@ -471,7 +498,7 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (w == 0) tmem_dealloc(tmem, kMom);
+    if (w == 0) tmem_dealloc(tmem, 2 * kMom);
 }
 
 template <bool COUNT, bool STACKLESS>
