@@ -17,7 +17,7 @@
 // accumulated (the third part of E measured 10 % slower for no gain within tolerance).  Thread t then reads its
 // own row of D, turns the moments about x0 into the moments about its mean (pair.cuh)
 // and adds its eleven gradient terms with FP32 atomics.  An MMA warp issues the products
-// while the consumers compute the next 16-row chunk (two A buffers); batches alternate
+// while the consumers compute the next 16-row chunks (three A buffers); batches alternate
 // between two TMEM accumulators, so that a batch's read-out waits until the next batch's
 // chunks are issued and its last MMAs drain meanwhile.
 #include "pair.cuh"
@@ -35,7 +35,7 @@ constexpr int kBChunks = kBRows / 16;  // K chunks of 16 rows
 constexpr int kMom = 32;               // B rows: 20 moment features + zero padding
 
 struct BwdSmem {
-    unsigned char A[2][2][kBBatch * 32];        // E chunk (128 x 16 bf16), two parts, two buffers
+    unsigned char A[3][2][kBBatch * 32];        // E chunk (128 x 16 bf16), two parts, three buffers
     unsigned char B[kBChunks][3][kMom * 32];    // Psi (32 x 16 bf16) per chunk, three parts
     float rx[kBRows], ry[kBRows], rz[kBRows];  // coordinates of the block's rows (pairs load as float2)
     uint8_t rok[kBRows];                        // W > 0.01 (pair statistics only)
@@ -43,7 +43,7 @@ struct BwdSmem {
     int2 desc[kBStages];                        // (count or -1 at the end, group)
     int stack[kStackCap];
     int tcand[kCandCap];
-    uint64_t full[kBStages], empty[kBStages], aready[2], afree[2], dready[2], dfree[2];
+    uint64_t full[kBStages], empty[kBStages], aready[3], afree[3], dready[2], dfree[2];
     uint32_t tmem_base;
 };
 
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
             mbar_init(&sm.full[s], 1);
             mbar_init(&sm.empty[s], 5);  // the four consumer warps and the MMA warp
         }
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < 3; b++) {
             mbar_init(&sm.aready[b], 4);
             mbar_init(&sm.afree[b], 1);
         }
@@ -252,8 +252,8 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 const uint32_t tmem_d = tmem + (n & 1u) * kMom;
                 bool ok = true;
                 for (int q = q0; q <= q1; q++, j++) {
-                    const int b = (int)(j & 1u);
-                    if (!mbar_wait(&sm.aready[b], (j >> 1) & 1u, status)) {
+                    const int b = (int)(j % 3u);
+                    if (!mbar_wait(&sm.aready[b], (j / 3u) & 1u, status)) {
                         ok = false;
                         break;
                     }
@@ -405,9 +405,9 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                          HZ = make_float2(g.hz + 0.0f, g.hz + 0.0f);
             bool okc = true;
             for (int q = q0; q <= q1; q++, j++) {
-                const int b = (int)(j & 1u);
-                if (j >= 2) {
-                    const bool okf = mbar_wait(&sm.afree[b], ((j >> 1) - 1) & 1u, status);
+                const int b = (int)(j % 3u);
+                if (j >= 3) {
+                    const bool okf = mbar_wait(&sm.afree[b], ((j / 3u) - 1) & 1u, status);
                     if (!__all_sync(0xffffffffu, okf)) {
                         okc = false;
                         break;
