@@ -9,7 +9,8 @@ Checks, with the tolerances of test_gpu_rasterizer:
 * at scale (200k clustered Gaussians x 1M samples) against the same backward walking the
   tree (log off): the same fields, gradients within the atomic-order tolerance;
 * a block with more candidates than its log slots (4096) falls back to walking;
-* a backward whose Gaussians are not the forward's (a different P) walks the tree.
+* a backward whose Gaussians are not the forward's (a different P) walks the tree;
+* a log recorded by the forward's stackless traversal serves the backward the same way.
 """
 import contextlib
 
@@ -145,3 +146,21 @@ def test_backward_of_other_gaussians_walks(cuda, orc, small_case):
     got = [x.cpu().numpy() for x in g]
     ref = oracle_backward(orc, sub, out.cpu().numpy(), outw.cpu().numpy(), c6.cpu().numpy().reshape(-1, 6), gout, gw)
     assert_grads_close(got, ref)
+
+
+def test_logged_backward_with_stackless_forward(cuda, orc, small_case):
+    """The stackless traversal hands the forward's producer the same candidates in another
+    order; the log it records serves the backward just the same."""
+    from bvh_diff_gaussian_rasterization import _C
+    S = small_case[-1].shape[0]
+    rng = np.random.default_rng(55)
+    gout = rng.normal(size=S).astype(np.float32)
+    gw = rng.normal(size=S).astype(np.float32)
+    _C.set_traversal("stackless")
+    try:
+        with modes():
+            got, out, outw, conics, st = step(cuda, small_case, gout, gw, count=True)
+    finally:
+        _C.set_traversal("stack")
+    assert st["bwd_node_visits"] == 0
+    assert_grads_close(got, oracle_backward(orc, small_case, out, outw, conics, gout, gw))
