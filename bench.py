@@ -222,6 +222,15 @@ def _oracle_path():
         sys.path.insert(0, p)
 
 
+def host_threads():
+    """Host threads the CPU arms use: every core this process may run on.  Set explicitly
+    because torch.distributed.run exports OMP_NUM_THREADS=1 to its ranks."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def cpu_kind():
     _oracle_path()
     import refslice
@@ -240,9 +249,11 @@ def cpu_step_time(kind, means, scales, rots, values, weights, samples, n_sub, se
         gt = target[pick]
     else:
         gt = (0.5 + 0.4 * np.sin(6 * sub[:, 0]) * np.sin(5 * sub[:, 1]) * np.sin(4 * sub[:, 2])).astype(np.float32)
+    nt = host_threads()
     t0 = time.perf_counter()
     if kind == "reference":
         import refslice
+        refslice.config(nthreads=nt)
         rc, rb = refslice.preprocess(means, scales, rots, weights)
         out, outw, _ = refslice.forward(means, values, weights, sub, rc, rb, use_gaussian_bvh=False)
         mask = out != -1
@@ -251,13 +262,13 @@ def cpu_step_time(kind, means, scales, rots, values, weights, samples, n_sub, se
                           np.zeros(n_sub, np.float32), use_gaussian_bvh=False)
     else:
         import oracle
-        c32, _, bb = oracle.preprocess(means, scales, rots, weights)
-        out, outw = oracle.forward(means, values, weights, c32.astype(np.float64), bb, sub)
+        c32, _, bb = oracle.preprocess(means, scales, rots, weights, nthreads=nt)
+        out, outw = oracle.forward(means, values, weights, c32.astype(np.float64), bb, sub, nthreads=nt)
         mask = out != -1
         g = np.where(mask, np.sign(out - gt), 0.0) / max(int(mask.sum()), 1)
         r = oracle.backward(means, values, weights, c32.astype(np.float64), bb, sub, out.astype(np.float32),
-                            outw.astype(np.float32), g.astype(np.float32), np.zeros(n_sub, np.float32))
-        oracle.cov_backward(scales, rots, c32, r["dconics"])
+                            outw.astype(np.float32), g.astype(np.float32), np.zeros(n_sub, np.float32), nthreads=nt)
+        oracle.cov_backward(scales, rots, c32, r["dconics"], nthreads=nt)
     return time.perf_counter() - t0
 
 
@@ -271,7 +282,7 @@ CPU_DESC = {"reference": "the reference's own kernels (diff-gaussian-rasterizati
 def cpu_extrapolated(kind, means, scales, rots, values, weights, samples, n_a, n_b, reps_b=1, warmup=0):
     """Times n_a points once and n_b points reps_b times (median) after `warmup` untimed
     n_b runs; extrapolates t = fixed + slope * S to the full step."""
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     S = samples.shape[0]
     tg = TARGETS.get("config2") if means.shape[0] == CONFIGS["config2"][0] and S == CONFIGS["config2"][1] else None
     t_a = cpu_step_time(kind, means, scales, rots, values, weights, samples, n_a, target=tg)
@@ -298,7 +309,7 @@ def cpu_baseline(means, scales, rots, values, weights, samples):
     kind = cpu_kind()
     S = samples.shape[0]
     if S <= 300_000:
-        threads = os.cpu_count() or 1
+        threads = host_threads()
         t = cpu_step_time(kind, means, scales, rots, values, weights, samples, S)
         return {"value": t * 1e3, "unit": "ms/step", "cores": threads, "kind": kind,
                 "sample": "%s: the full step, all %d points and %d Gaussians" % (CPU_DESC[kind], S, means.shape[0]),
@@ -393,7 +404,7 @@ def run_reference(args):
         t = [cpu_step_time(kind, means, scales, rots, values, weights, samples, S, seed=10 + k)
              for k in range(args.steps)]
         full_ms = float(np.median(t)) * 1e3
-        cpu = {"value": full_ms, "unit": "ms/step", "cores": os.cpu_count() or 1, "kind": kind,
+        cpu = {"value": full_ms, "unit": "ms/step", "cores": host_threads(), "kind": kind,
                "sample": "%s: the full step (all %d points, %d Gaussians), median of %d" %
                          (CPU_DESC[kind], S, means.shape[0], args.steps), "extrapolated": False}
         extra = {"extrapolated": False}
@@ -471,9 +482,9 @@ def mesh_bench(dev, steps, warmup, with_cpu):
         import oracle
         sub = q[:1_000_000]
         t0 = time.perf_counter()
-        r_out, r_cell = oracle.sample_tets(pts, tets, vals, sub)
+        r_out, r_cell = oracle.sample_tets(pts, tets, vals, sub, nthreads=host_threads())
         t = time.perf_counter() - t0
-        tet["cpu_oracle"] = {"points_per_s": sub.shape[0] / t, "cores": os.cpu_count() or 1,
+        tet["cpu_oracle"] = {"points_per_s": sub.shape[0] / t, "cores": host_threads(),
                              "sample": "oracle (C, OpenMP, uniform grid locator) on 1M of the points, "
                                        "locator build included (%.2f s)" % t}
         g_out = d_out[:sub.shape[0]].cpu().numpy()
@@ -499,9 +510,9 @@ def mesh_bench(dev, steps, warmup, with_cpu):
     del d_bs, d_bg
     if with_cpu:
         t0 = time.perf_counter()
-        oracle.training_samples(pts, tets, vals, 1, 2_000_000, seed=0)
+        oracle.training_samples(pts, tets, vals, 1, 2_000_000, seed=0, nthreads=host_threads())
         t = time.perf_counter() - t0
-        tb["cpu_oracle"] = {"points_per_s": 2_000_000 / t, "cores": os.cpu_count() or 1,
+        tb["cpu_oracle"] = {"points_per_s": 2_000_000 / t, "cores": host_threads(),
                             "sample": "oracle (C Philox points, numpy stable Morton sort, C grid locator) on "
                                       "one batch of 2M points (%.2f s)" % t}
     res["training_batches"] = tb
@@ -729,10 +740,10 @@ def knn_bench(dev, means, steps, warmup, with_cpu):
         import oracle
         host = pts.cpu().numpy()
         t0 = time.perf_counter()
-        ref = oracle.knn3_mean_dist2(host)
+        ref = oracle.knn3_mean_dist2(host, nthreads=host_threads())
         t = time.perf_counter() - t0
         res["bit_exact_vs_oracle"] = bool(np.array_equal(ref, out.cpu().numpy()))
-        res["cpu_oracle"] = {"ms_per_call": t * 1e3, "cores": os.cpu_count() or 1,
+        res["cpu_oracle"] = {"ms_per_call": t * 1e3, "cores": host_threads(),
                              "sample": "oracle (C, OpenMP, uniform grid) on all %d points" % n}
     return res
 
