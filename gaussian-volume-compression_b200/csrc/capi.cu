@@ -428,11 +428,18 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
         // the candidates are logged for the tensor-core backward when it is the one selected
         const bool tc_bwd = ctx->bwd_mode == 3 || (ctx->bwd_mode == 0 && ctx->eval_path == 1);
         if (tc_bwd && ctx->cand_log && ctx->S > 0) {
+            // 16 KB per 128 samples: where that does not fit in device memory, the forward
+            // runs without the log and the backward walks the tree
             const int64_t n_blocks = (ctx->S + 127) / 128;
-            GVC_CUDA(ctx->clog.ensure(sizeof(int32_t) * kCandLogPerBlock * n_blocks), "alloc candidate log");
-            GVC_CUDA(ctx->cend.ensure(sizeof(int32_t) * 8 * n_blocks), "alloc candidate log ends");
-            ca.clog = ctx->clog.as<int32_t>();
-            ca.cend = ctx->cend.as<int32_t>();
+            if (ctx->clog.ensure(sizeof(int32_t) * kCandLogPerBlock * n_blocks) == cudaSuccess &&
+                ctx->cend.ensure(sizeof(int32_t) * 8 * n_blocks) == cudaSuccess) {
+                ca.clog = ctx->clog.as<int32_t>();
+                ca.cend = ctx->cend.as<int32_t>();
+            } else {
+                (void)cudaGetLastError();  // a failed allocation is not sticky: clear it
+                ctx->clog.release();
+                ctx->cend.release();
+            }
         }
         GVC_CUDA(launch_forward_cta(ca, ctx->eval_path == 1, st), "forward (CTA)");
         ctx->clog_ready = ca.clog != nullptr;

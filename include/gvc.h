@@ -72,7 +72,9 @@ typedef enum {
                                backward reads them back instead of walking the Gaussian LBVH
                                again (each of its finer block groups keeps the candidates of
                                the enclosing forward group whose boxes overlap its own);
-                               blocks with more candidates are walked.  0 = always walk.   */
+                               blocks with more candidates are walked, and without device
+                               memory for the log the forward runs without it.
+                               0 = always walk.                                            */
 } gvc_option;
 
 typedef struct {
