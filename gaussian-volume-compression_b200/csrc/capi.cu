@@ -143,11 +143,14 @@ int debug_check(gvc_ctx* ctx, cudaStream_t st) {
     if (e != cudaSuccess) return cuda_fail(ctx, e, "debug synchronize");
     e = cudaMemcpy(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "status copy");
-    if (*ctx->h_status & kStatusStackOverflow) {
-        cudaMemset(ctx->d_status, 0, sizeof(int));
+    const int s = *ctx->h_status;
+    if (s == 0) return GVC_OK;
+    e = cudaMemset(ctx->d_status, 0, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "status clear");
+    if (s & kStatusStackOverflow)
         return fail(ctx, GVC_ERR_TRAVERSAL, "BVH traversal stack overflow: results are invalid");
-    }
-    return GVC_OK;
+    return fail(ctx, GVC_ERR_TIMEOUT,
+                "a bounded device-side wait ran out (pipeline barrier or radix-sort look-back): results are invalid");
 }
 
 }  // namespace
@@ -176,6 +179,9 @@ int gvc_ctx_create(gvc_ctx** out) {
     GVC_CUDA(cudaMalloc(&c->d_stats, sizeof(unsigned long long) * 16), "cudaMalloc stats");
     GVC_CUDA(cudaMemset(c->d_stats, 0, sizeof(unsigned long long) * 16), "cudaMemset stats");
     GVC_CUDA(cudaMallocHost(&c->h_status, sizeof(int)), "cudaMallocHost");
+    Lbvh* sorted[] = {&c->s_sort, &c->tiles, &c->gbvh, &c->cells, &c->knn, &c->ts_sort, &c->scratch.dbg,
+                      &c->scratch.msamp};
+    for (Lbvh* L : sorted) L->status = c->d_status;
     *out = c;
     return GVC_OK;
 }
@@ -190,7 +196,8 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
                      &c->knn,     &c->ts_sort,    &c->scratch.dbg,   &c->scratch.msamp};
     for (Lbvh* L : lbvhs) {
         DevBuf* bufs[] = {&L->keys, &L->keys_alt, &L->perm, &L->perm_alt, &L->boxes, &L->sorted_boxes, &L->left,
-                          &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds};
+                          &L->right, &L->parent, &L->flags, &L->node_boxes, &L->nodes, &L->hist, &L->bounds,
+                          &L->onesweep};
         for (DevBuf* b : bufs) b->release();
     }
     DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->blk_desc_b, &c->blk_boxes_b, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
@@ -788,6 +795,12 @@ int gvc_debug_tc_gemm(gvc_ctx* ctx, const void* A, const void* B, int N, float* 
     if (N < 32 || N > 256 || N % 32) return fail(ctx, GVC_ERR_ARG, "N must be a multiple of 32 in [32, 256]");
     if (!A || !B || !D) return fail(ctx, GVC_ERR_ARG, "null pointer");
     GVC_CUDA(launch_tc_gemm_test(A, B, N, D, ctx->d_status, (cudaStream_t)stream), "tc gemm");
+    return GVC_OK;
+}
+
+int gvc_debug_wait_timeout(gvc_ctx* ctx, void* stream) {
+    if (!ctx) return GVC_ERR_ARG;
+    GVC_CUDA(launch_wait_timeout_test(ctx->d_status, (cudaStream_t)stream), "wait timeout");
     return GVC_OK;
 }
 

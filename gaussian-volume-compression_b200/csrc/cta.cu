@@ -63,9 +63,12 @@ __device__ __forceinline__ Box6 rows_box(int a, int b, const float (&x)[4], cons
 
 // Split row of [a, b) or -1 (warp-uniform): at the first Morton bit where the range's
 // first and last keys differ, taken when both halves' boxes have at most half the
-// half-perimeter of the whole.
-__device__ int rows_split(int a, int b, const uint32_t* keys, const uint32_t (&key)[4], const float (&x)[4],
-                          const float (&y)[4], const float (&z)[4], float ratio) {
+// half-perimeter of the whole.  B is the box of [a, b); on a split B1 and B2 receive the
+// boxes of the two halves (box unions are exact, so a box computed once for a range is
+// the box of that range wherever it is used).
+__device__ int rows_split(int a, int b, const Box6& B, Box6& B1, Box6& B2, const uint32_t* keys,
+                          const uint32_t (&key)[4], const float (&x)[4], const float (&y)[4], const float (&z)[4],
+                          float ratio) {
     if (b - a < 2) return -1;
     const uint32_t ka = keys[a], kb = keys[b - 1];
     if (ka == kb) return -1;
@@ -80,19 +83,24 @@ __device__ int rows_split(int a, int b, const uint32_t* keys, const uint32_t (&k
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, off));
     const int m = first;
-    const Box6 B = rows_box(a, b, x, y, z);
-    const Box6 B1 = rows_box(a, m, x, y, z);
-    const Box6 B2 = rows_box(m, b, x, y, z);
+    B1 = rows_box(a, m, x, y, z);
+    B2 = rows_box(m, b, x, y, z);
     return fmaxf(hp6(B1), hp6(B2)) <= ratio * hp6(B) ? m : -1;
 }
 
 constexpr int kBlocksPerCta = 8;  // 128-row blocks (warps) per CTA of k_sample_blocks
 
-// Splits the block's valid rows [0, nvalid) three times (every range of a level in
-// order, at most 8 groups) with `ratio` and writes bdesc[blk] = (starts of groups 1..7
-// as bytes, 128 if unused; byte 7 = group count) and bboxes[blk * 8 + g] = (lo, hi) of
-// group g (empty box if unused).
-__device__ __forceinline__ void block_split_store(int64_t blk, int nvalid, const uint32_t* keys,
+__device__ __forceinline__ Box6 shfl_box(const Box6& b, int src) {
+    return Box6{__shfl_sync(0xffffffffu, b.lx, src), __shfl_sync(0xffffffffu, b.ly, src),
+                __shfl_sync(0xffffffffu, b.lz, src), __shfl_sync(0xffffffffu, b.hx, src),
+                __shfl_sync(0xffffffffu, b.hy, src), __shfl_sync(0xffffffffu, b.hz, src)};
+}
+
+// Splits the block's valid rows [0, nvalid) (box B0) three times (every range of a level
+// in order, at most 8 groups) with `ratio` and writes bdesc[blk] = (starts of groups
+// 1..7 as bytes, 128 if unused; byte 7 = group count) and bboxes[blk * 8 + g] = (lo, hi)
+// of group g (empty box if unused).  The box of range i of a level is held by lane i.
+__device__ __forceinline__ void block_split_store(int64_t blk, int nvalid, const Box6& B0, const uint32_t* keys,
                                                   const uint32_t (&key)[4], const float (&x)[4],
                                                   const float (&y)[4], const float (&z)[4], float ratio,
                                                   uint2* __restrict__ bdesc, float4* __restrict__ bboxes) {
@@ -101,17 +109,24 @@ __device__ __forceinline__ void block_split_store(int64_t blk, int nvalid, const
     int nr = 1;
     ra[0] = 0;
     rb[0] = nvalid;
+    Box6 lb = B0;  // lane i: box of range i
     for (int depth = 0; depth < 3; depth++) {
         int na[kBlockGroups], nbb[kBlockGroups];
+        Box6 nlb = lb;
         int nn = 0;
         for (int i = 0; i < nr; i++) {
-            const int m = rows_split(ra[i], rb[i], keys, key, x, y, z, ratio);
+            const Box6 Bi = shfl_box(lb, i);
+            Box6 B1, B2;
+            const int m = rows_split(ra[i], rb[i], Bi, B1, B2, keys, key, x, y, z, ratio);
             if (m >= 0) {
+                if (lane == nn) nlb = B1;
                 na[nn] = ra[i];
                 nbb[nn++] = m;
+                if (lane == nn) nlb = B2;
                 na[nn] = m;
                 nbb[nn++] = rb[i];
             } else {
+                if (lane == nn) nlb = Bi;
                 na[nn] = ra[i];
                 nbb[nn++] = rb[i];
             }
@@ -120,19 +135,18 @@ __device__ __forceinline__ void block_split_store(int64_t blk, int nvalid, const
             ra[i] = na[i];
             rb[i] = nbb[i];
         }
+        lb = nlb;
         nr = nn;
     }
-    uint32_t starts[kBlockGroups];
-    for (int g = 0; g < kBlockGroups; g++) starts[g] = g < nr ? (uint32_t)ra[g] : (uint32_t)kBlockRows;
-    for (int g = 0; g < kBlockGroups; g++) {
+    if (lane < kBlockGroups) {
         Box6 B{INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-        if (g < nr) B = rows_box(ra[g], rb[g], x, y, z);
-        if (lane == 0) {
-            bboxes[2 * (blk * kBlockGroups + g)] = make_float4(B.lx, B.ly, B.lz, 0.f);
-            bboxes[2 * (blk * kBlockGroups + g) + 1] = make_float4(B.hx, B.hy, B.hz, 0.f);
-        }
+        if (lane < nr) B = lb;
+        bboxes[2 * (blk * kBlockGroups + lane)] = make_float4(B.lx, B.ly, B.lz, 0.f);
+        bboxes[2 * (blk * kBlockGroups + lane) + 1] = make_float4(B.hx, B.hy, B.hz, 0.f);
     }
     if (lane == 0) {
+        uint32_t starts[kBlockGroups];
+        for (int g = 0; g < kBlockGroups; g++) starts[g] = g < nr ? (uint32_t)ra[g] : (uint32_t)kBlockRows;
         uint2 d;
         d.x = starts[1] | (starts[2] << 8) | (starts[3] << 16) | (starts[4] << 24);
         d.y = starts[5] | (starts[6] << 8) | (starts[7] << 16) | ((uint32_t)nr << 24);
@@ -172,8 +186,9 @@ __global__ void __launch_bounds__(32 * kBlocksPerCta) k_sample_blocks(const floa
     __syncwarp();
     const int64_t rem = S - blk * kBlockRows;
     const int nvalid = rem < kBlockRows ? (int)rem : kBlockRows;
-    block_split_store(blk, nvalid, keys, key, x, y, z, ratio, bdesc, bboxes);
-    if (bdesc2) block_split_store(blk, nvalid, keys, key, x, y, z, ratio2, bdesc2, bboxes2);
+    const Box6 B0 = rows_box(0, nvalid, x, y, z);
+    block_split_store(blk, nvalid, B0, keys, key, x, y, z, ratio, bdesc, bboxes);
+    if (bdesc2) block_split_store(blk, nvalid, B0, keys, key, x, y, z, ratio2, bdesc2, bboxes2);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -567,6 +582,23 @@ cudaError_t launch_forward_cta(const CtaArgs& a, bool tc, cudaStream_t st) {
 cudaError_t launch_tc_gemm_test(const void* A, const void* B, int N, float* D, int* status, cudaStream_t st) {
     k_tc_gemm_test<<<1, 128, 0, st>>>(reinterpret_cast<const __nv_bfloat16*>(A),
                                       reinterpret_cast<const __nv_bfloat16*>(B), N, D, status); gvc::note_launch();
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(32) k_wait_timeout_test(int* status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    // nothing arrives on `bar`: phase 0 never completes and the wait gives up
+    if (threadIdx.x == 0) (void)mbar_wait(&bar, 0, status);
+    __syncwarp();
+}
+
+cudaError_t launch_wait_timeout_test(int* status, cudaStream_t st) {
+    k_wait_timeout_test<<<1, 32, 0, st>>>(status); gvc::note_launch();
     return cudaGetLastError();
 }
 

@@ -27,6 +27,7 @@ void note_launch(int n = 1);
 
 // Device status bits (OR-ed into ctx->d_status).
 constexpr int kStatusStackOverflow = 1;
+constexpr int kStatusTimeout = 2;  // a bounded wait gave up (mbarrier, radix-sort look-back)
 
 // Gaussian evaluation record, one per Gaussian in LBVH (Morton) order: 80 bytes.
 //   r0 = (mu.x, mu.y, mu.z, w)
@@ -86,6 +87,8 @@ struct Lbvh {
     DevBuf node_boxes;                      // [n-1] internal node boxes, 2 x float4
     DevBuf nodes;                           // [n-1] BvhNode
     DevBuf hist, bounds;                    // sort histograms, centroid bounds
+    DevBuf onesweep;                        // one-kernel-per-pass sort: digit counts, tickets, look-back words
+    int* status = nullptr;                  // device status word; null keeps the three-kernel sort passes
 };
 
 }  // namespace gvc

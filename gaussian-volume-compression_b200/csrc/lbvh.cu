@@ -301,9 +301,263 @@ __global__ void __launch_bounds__(256) k_rs_scatter(const uint32_t* __restrict__
     }
 }
 
+// ----------------------------------------------------------------------------------
+// One kernel per pass (the onesweep scheme of Adinets & Merrill 2022): the digit counts
+// of all four passes come from one read of the keys (k_os_hist); in each pass the tiles
+// take tickets in the order their blocks start, rank their keys as k_rs_scatter does,
+// publish their per-digit counts and find the counts of every tile before them by
+// decoupled look-back (Merrill & Garland 2016): the words of the preceding tiles are
+// read from the nearest backwards, adding aggregates until an inclusive prefix is met.
+// A word packs a 2-bit state (not ready / aggregate / inclusive) with a 30-bit count, so
+// n < 2^30.  A tile only waits on tiles with smaller tickets, whose blocks are already
+// running and wait only on tiles before their own, so the look-back ends; its spin is
+// bounded all the same (kStatusTimeout, results invalid).  Same stable order as the
+// three-kernel passes: tile t holds keys [t * kRsTile, (t + 1) * kRsTile) of the pass's
+// input whatever block takes ticket t.
+// ----------------------------------------------------------------------------------
+constexpr uint32_t kOsAggregate = 1u << 30;
+constexpr uint32_t kOsInclusive = 2u << 30;
+constexpr uint32_t kOsCount = (1u << 30) - 1u;
+constexpr long long kOsSpinCycles = 200000000LL;  // ~0.1 s at 2 GHz
+constexpr int kOsWindow = 16;                    // look-back words read per round trip
+
+__device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// ghist[pass * 256 + digit] += count over keys[0, n) (ghist zeroed by the caller).
+__global__ void __launch_bounds__(256) k_os_hist(const uint32_t* __restrict__ keys, int64_t n,
+                                                 uint32_t* __restrict__ ghist) {
+    __shared__ uint32_t cnt[4 * 256];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) cnt[i] = 0u;
+    __syncthreads();
+    const int64_t nv = n >> 2;  // uint4 loads (the buffer is 256-byte aligned), then the tail
+    const uint4* k4 = reinterpret_cast<const uint4*>(keys);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv + 4; i += stride) {
+        uint32_t k[4];
+        int m = 0;
+        if (i < nv) {
+            const uint4 q = k4[i];
+            k[0] = q.x;
+            k[1] = q.y;
+            k[2] = q.z;
+            k[3] = q.w;
+            m = 4;
+        } else if (4 * nv + (i - nv) < n) {
+            k[0] = keys[4 * nv + (i - nv)];
+            m = 1;
+        }
+        for (int j = 0; j < m; j++) {
+            atomicAdd(&cnt[k[j] & 255u], 1u);
+            atomicAdd(&cnt[256 + ((k[j] >> 8) & 255u)], 1u);
+            atomicAdd(&cnt[512 + ((k[j] >> 16) & 255u)], 1u);
+            atomicAdd(&cnt[768 + (k[j] >> 24)], 1u);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+        const uint32_t v = cnt[i];
+        if (v) atomicAdd(&ghist[i], v);
+    }
+}
+
+__global__ void __launch_bounds__(256, 4) k_os_scatter(const uint32_t* __restrict__ keys_in,
+                                                    const int32_t* __restrict__ vals_in,
+                                                    uint32_t* __restrict__ keys_out, int32_t* __restrict__ vals_out,
+                                                    int64_t n, int pass, const uint32_t* __restrict__ ghist,
+                                                    uint32_t* __restrict__ look, uint32_t* __restrict__ ticket,
+                                                    int* __restrict__ status) {
+    __shared__ uint32_t wcnt[kRsWarps][256];
+    __shared__ uint32_t dbase[256];
+    __shared__ uint32_t bstart[256];
+    __shared__ uint32_t wsum[kRsWarps];
+    __shared__ uint32_t skey[kRsTile];
+    __shared__ int32_t sval[kRsTile];
+    __shared__ uint32_t s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int shift = 8 * pass;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    for (int t = threadIdx.x; t < kRsWarps * 256; t += blockDim.x) (&wcnt[0][0])[t] = 0;
+    // first position of each digit in the output: exclusive scan of the pass's digit counts
+    if (warp == 0) {
+        uint32_t run = 0;
+        for (int chunk = 0; chunk < 8; chunk++) {
+            const int d = chunk * 32 + lane;
+            const uint32_t v = ghist[pass * 256 + d];
+            uint32_t incl = v;
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += t;
+            }
+            dbase[d] = run + incl - v;
+            run += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    }
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int64_t base = tile * kRsTile + (int64_t)warp * (kRsIters * 32);
+    uint32_t kreg[kRsIters];
+    int32_t vreg[kRsIters];
+    uint32_t rreg[kRsIters];  // (local rank << 8) | digit, or 0xffffffff if invalid
+#pragma unroll
+    for (int it = 0; it < kRsIters; it++) {
+        const int64_t idx = base + it * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t key = valid ? keys_in[idx] : 0u;
+        const int32_t val = valid ? (vals_in ? vals_in[idx] : (int32_t)idx) : 0;
+        const uint32_t d = (key >> shift) & 255u;
+        const uint32_t tag = valid ? d : (256u + lane);
+        const uint32_t peers = __match_any_sync(0xffffffffu, tag);
+        const uint32_t rank = __popc(peers & lanemask_lt());
+        const uint32_t pre = valid ? wcnt[warp][d] : 0u;
+        __syncwarp();
+        if (valid && (__ffs(peers) - 1) == lane) wcnt[warp][d] = pre + __popc(peers);
+        __syncwarp();
+        kreg[it] = key;
+        vreg[it] = val;
+        rreg[it] = valid ? (((pre + rank) << 8) | d) : 0xffffffffu;
+    }
+    __syncthreads();
+    // exclusive prefix over warps for each digit; run = this tile's count of digit d
+    const int d = threadIdx.x;  // 256 threads == 256 digits
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kRsWarps; w++) {
+        const uint32_t t = wcnt[w][d];
+        wcnt[w][d] = run;
+        run += t;
+    }
+    // publish this tile's count of digit d at once, so that later tiles can pass over it
+    uint32_t* mine = look + tile * 256 + d;
+    st_relaxed_gpu(mine, (tile == 0 ? kOsInclusive : kOsAggregate) | run);
+    // tile-local start of each digit: exclusive scan of the 256 counts
+    {
+        uint32_t incl = run;
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += t;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t wbase = 0;
+        for (int w = 0; w < warp; w++) wbase += wsum[w];
+        bstart[threadIdx.x] = wbase + incl - run;
+    }
+    __syncthreads();
+    // the keys go to their tile-local sorted slots before the look-back (their registers
+    // are free for the look-back's window)
+#pragma unroll
+    for (int it = 0; it < kRsIters; it++) {
+        const uint32_t r = rreg[it];
+        if (r != 0xffffffffu) {
+            const uint32_t dd = r & 255u;
+            const uint32_t sp = bstart[dd] + wcnt[warp][dd] + (r >> 8);
+            skey[sp] = kreg[it];
+            sval[sp] = vreg[it];
+        }
+    }
+    // look back for the count of digit d in all tiles before this one, kOsWindow words
+    // per round trip: aggregates are added until an inclusive prefix is met; a tile not
+    // ready yet stops the round (the words before it are kept) and is read again
+    if (tile > 0) {
+        uint32_t excl = 0;
+        int64_t k = tile - 1;  // nearest tile not accounted for yet
+        const long long t0 = clock64();
+        bool ok = true;
+        while (true) {
+            uint32_t v[kOsWindow];
+#pragma unroll
+            for (int i = 0; i < kOsWindow; i++) v[i] = k - i >= 0 ? ld_relaxed_gpu(look + (k - i) * 256 + d) : kOsInclusive;
+            uint32_t add = 0;
+            int taken = 0;
+            bool inclusive = false, blocked = false;
+#pragma unroll
+            for (int i = 0; i < kOsWindow; i++) {
+                if (!inclusive && !blocked) {
+                    const uint32_t state = v[i] & ~kOsCount;
+                    if (state == 0u) {
+                        blocked = true;
+                    } else {
+                        add += v[i] & kOsCount;
+                        taken++;
+                        inclusive = state == kOsInclusive;
+                    }
+                }
+            }
+            excl += add;
+            if (inclusive) break;
+            k -= taken;
+            if (blocked) {
+                if (clock64() - t0 > kOsSpinCycles) {
+                    ok = false;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        if (!ok) atomicOr(status, kStatusTimeout);
+        st_relaxed_gpu(mine, kOsInclusive | ((excl + run) & kOsCount));
+        dbase[d] += excl;
+    }
+    __syncthreads();
+    const int64_t rem = n - tile * kRsTile;
+    const int cnt = rem < kRsTile ? (int)rem : kRsTile;
+    for (int sp = threadIdx.x; sp < cnt; sp += blockDim.x) {
+        const uint32_t key = skey[sp];
+        const uint32_t dd = (key >> shift) & 255u;
+        const uint32_t pos = dbase[dd] + ((uint32_t)sp - bstart[dd]);
+        // pos < n always (a timed-out look-back only undercounts); the test costs nothing
+        if (pos < (uint64_t)n) {
+            keys_out[pos] = key;
+            vals_out[pos] = sval[sp];
+        }
+    }
+}
+
+static cudaError_t radix_sort_onesweep(Lbvh& L, int64_t n, cudaStream_t st) {
+    const int64_t T = (n + kRsTile - 1) / kRsTile;
+    const size_t head = sizeof(uint32_t) * (4 * 256 + 64);  // digit counts [4][256], tickets [4] (padded)
+    const size_t look = sizeof(uint32_t) * 256 * (size_t)T;  // one word per (tile, digit) and pass
+    cudaError_t e;
+    if ((e = L.keys_alt.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.perm.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.perm_alt.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;
+    if ((e = L.onesweep.ensure(head + 4 * look)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(L.onesweep.ptr, 0, head + 4 * look, st)) != cudaSuccess) return e;
+    uint32_t* ghist = L.onesweep.as<uint32_t>();
+    uint32_t* tickets = ghist + 4 * 256;
+    uint32_t* look0 = ghist + head / sizeof(uint32_t);
+    const unsigned hb = (unsigned)(T < 148 * 4 ? T : 148 * 4);
+    k_os_hist<<<hb, 256, 0, st>>>(L.keys.as<uint32_t>(), n, ghist); gvc::note_launch();
+    uint32_t* kin = L.keys.as<uint32_t>();
+    uint32_t* kout = L.keys_alt.as<uint32_t>();
+    int32_t* vin = nullptr;
+    int32_t* vout = L.perm_alt.as<int32_t>();
+    for (int pass = 0; pass < 4; pass++) {
+        k_os_scatter<<<(unsigned)T, 256, 0, st>>>(kin, vin, kout, vout, n, pass, ghist,
+                                                  look0 + (size_t)pass * 256 * (size_t)T, tickets + pass,
+                                                  L.status); gvc::note_launch();
+        // ping-pong as in radix_sort_pairs: the result ends in L.keys / L.perm
+        uint32_t* tk = kin;
+        kin = kout;
+        kout = tk;
+        vin = vout;
+        vout = (vout == L.perm_alt.as<int32_t>()) ? L.perm.as<int32_t>() : L.perm_alt.as<int32_t>();
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t radix_sort_pairs(Lbvh& L, int64_t n, cudaStream_t st) {
     // Input: L.keys [n]. Output: L.keys sorted, L.perm (sorted pos -> input index).
     if (n <= 0) return cudaSuccess;
+    // one kernel per pass where a status word can take the look-back's timeout report
+    if (L.status && n <= (int64_t)kOsCount) return radix_sort_onesweep(L, n, st);
     const int nb = (int)((n + kRsTile - 1) / kRsTile);
     cudaError_t e;
     if ((e = L.keys_alt.ensure(LbvhBytes::keys(n))) != cudaSuccess) return e;

@@ -114,6 +114,9 @@ cudaError_t launch_forward_cta(const CtaArgs& a, bool tc, cudaStream_t st);
 // fwd_tc.cu: the forward with the exponent on tcgen05 (launch_forward_cta(a, true) calls it)
 cudaError_t launch_forward_tc(const CtaArgs& a, cudaStream_t st);
 cudaError_t launch_tc_gemm_test(const void* A, const void* B, int N, float* D, int* status, cudaStream_t st);
+// One block waiting on an mbarrier nothing arrives on: the bounded wait runs out and
+// records kStatusTimeout (tests the host-side report of device timeouts).
+cudaError_t launch_wait_timeout_test(int* status, cudaStream_t st);
 cudaError_t launch_backward_gauss(const BwdArgs& a, cudaStream_t st);
 // bwd_tc.cu: backward on 128-sample blocks with the reduction over samples on tcgen05
 cudaError_t launch_backward_cta(const BwdArgs& a, int64_t n_blocks, const uint2* bdesc, const float4* bboxes,

@@ -14,7 +14,6 @@
 
 namespace gvc {
 
-constexpr int kStatusTimeout = 2;
 // Bounded spin for mbarrier waits: ~0.1 s at 2 GHz.
 constexpr long long kSpinCycles = 200000000LL;
 

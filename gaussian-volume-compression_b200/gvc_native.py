@@ -13,9 +13,10 @@ LIB_PATH = os.path.join(_HERE, "libgvc.so")
 
 GVC_OK = 0
 GVC_ERR_TRAVERSAL = 4
+GVC_ERR_TIMEOUT = 7
 STATUS_NAMES = {
     0: "GVC_OK", 1: "GVC_ERR_ARG", 2: "GVC_ERR_CUDA", 3: "GVC_ERR_CAPACITY",
-    4: "GVC_ERR_TRAVERSAL", 5: "GVC_ERR_UNSUPPORTED", 6: "GVC_ERR_STATE",
+    4: "GVC_ERR_TRAVERSAL", 5: "GVC_ERR_UNSUPPORTED", 6: "GVC_ERR_STATE", 7: "GVC_ERR_TIMEOUT",
 }
 OPT_COV_GRAD, OPT_BWD_MODE, OPT_EVAL_PATH, OPT_COUNT_PAIRS, OPT_TIME_KERNELS, OPT_TRAVERSAL = 1, 2, 3, 4, 5, 6
 OPT_CAND_LOG = 7
@@ -50,6 +51,7 @@ _SIGNATURES = {
     "gvc_debug_preprocess": [_vp, _i64, _vp, _vp, _vp, _vp, _f32, _vp, _vp, _vp],
     "gvc_debug_sample_order": [_vp, _vp, _vp, _vp],
     "gvc_debug_tc_gemm": [_vp, _vp, _vp, _int, _vp, _vp],
+    "gvc_debug_wait_timeout": [_vp, _vp],
     "gvc_sample_tets_static": [_i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i64],
 }
 _RESTYPES = {"gvc_ctx_destroy": None, "gvc_last_error": ctypes.c_char_p, "gvc_launch_count": ctypes.c_int64}

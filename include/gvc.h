@@ -31,7 +31,8 @@ typedef enum {
     GVC_ERR_CAPACITY = 3,    /* a size exceeds a documented maximum                   */
     GVC_ERR_TRAVERSAL = 4,   /* a BVH traversal stack overflowed (results invalid)    */
     GVC_ERR_UNSUPPORTED = 5, /* unsupported cell type / dtype                         */
-    GVC_ERR_STATE = 6        /* call order violated (forward before build_bvh, ...)   */
+    GVC_ERR_STATE = 6,       /* call order violated (forward before build_bvh, ...)   */
+    GVC_ERR_TIMEOUT = 7      /* a bounded device-side wait ran out (results invalid) */
 } gvc_status;
 
 /* Options for gvc_set_option. */
@@ -107,7 +108,9 @@ int gvc_get_stats(gvc_ctx* ctx, gvc_stats* out, void* stream); /* synchronises `
 /* Number of kernel launches this library has issued in the process so far (all
    contexts); no counterpart in the reference. */
 int64_t gvc_launch_count(void);
-/* Waits for `stream`, returns the device status word (GVC_OK or GVC_ERR_TRAVERSAL) and clears it. */
+/* Waits for `stream`, returns the device status word (GVC_OK, GVC_ERR_TRAVERSAL, or
+   GVC_ERR_TIMEOUT when a kernel's bounded wait on a pipeline barrier or on another
+   block's published count ran out) and clears it. */
 int gvc_sync_status(gvc_ctx* ctx, void* stream);
 
 /* Replaces BuildBVH (diff-gaussian-rasterization/ext.cu:28-65).
@@ -236,6 +239,12 @@ int gvc_debug_preprocess(gvc_ctx* ctx, int64_t P, const float* means3D, const fl
    the tensor cores (tcgen05.mma, one CTA); N a multiple of 32 in [32, 256]; row-major
    device arrays.  No counterpart in the reference. */
 int gvc_debug_tc_gemm(gvc_ctx* ctx, const void* A, const void* B, int N, float* D, void* stream);
+
+/* Test hook: one block waits on a pipeline barrier (mbarrier) that nothing completes,
+   with the same bounded wait as the evaluation kernels (about 0.1 s), records the
+   timeout in the device status word and returns; the next gvc_sync_status reports
+   GVC_ERR_TIMEOUT.  No counterpart in the reference. */
+int gvc_debug_wait_timeout(gvc_ctx* ctx, void* stream);
 
 /* Test hook: the sample ordering of the last gvc_build_bvh: perm [S] int32 (sorted
    position -> caller index) and keys [S] uint32. */
