@@ -404,7 +404,6 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
             const float2 HX = make_float2(g.hx + 0.0f, g.hx + 0.0f), HY = make_float2(g.hy + 0.0f, g.hy + 0.0f),
                          HZ = make_float2(g.hz + 0.0f, g.hz + 0.0f);
             bool okc = true;
-            const bool wempty = 32 * w >= d.x;  // warp-uniform
             for (int q = q0; q <= q1; q++, j++) {
                 const int b = (int)(j % 3u);
                 if (j >= 3) {
@@ -420,48 +419,44 @@ __global__ void __launch_bounds__(kBRows + 64, 4) k_backward_cta(
                 const int c0 = max(ra - 16 * q, 0), c1 = min(rb - 16 * q, 16);
                 const uint32_t rmask = c1 > c0 ? (((1u << (c1 - c0)) - 1u) << c0) : 0u;
                 // Rows two at a time: the coordinates load as float2 pairs and the power runs
-                // on packed f32x2 FMAs (the AABB test, window and ex2 per row).  A warp none of
-                // whose lanes holds a Gaussian of this batch (the tail of a group's last batch)
-                // only writes its zero rows of E.
-                uint32_t hw[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u}, mw[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
-                if (!wempty) {
+                // on packed f32x2 FMAs (the AABB test, window and ex2 per row).
+                uint32_t hw[8], mw[8];
 #pragma unroll
-                    for (int k = 0; k < 16; k += 2) {
-                        const int r = 16 * q + k;
-                        const float2 X = *reinterpret_cast<const float2*>(&sm.rx[r]);
-                        const float2 Y = *reinterpret_cast<const float2*>(&sm.ry[r]);
-                        const float2 Z = *reinterpret_cast<const float2*>(&sm.rz[r]);
-                        // rows of the chunk outside the group need no mask: their Psi rows are zero
-                        const float2 M1 = make_float2(-1.0f, -1.0f);
-                        const float2 lx2 = __fadd2_rn(X, NLX), ly2 = __fadd2_rn(Y, NLY), lz2 = __fadd2_rn(Z, NLZ);
-                        const float2 hx2 = __ffma2_rn(X, M1, HX), hy2 = __ffma2_rn(Y, M1, HY), hz2 = __ffma2_rn(Z, M1, HZ);
-                        const uint32_t b0 = __float_as_uint(lx2.x) | __float_as_uint(ly2.x) | __float_as_uint(lz2.x) |
-                                            __float_as_uint(hx2.x) | __float_as_uint(hy2.x) | __float_as_uint(hz2.x);
-                        const uint32_t b1 = __float_as_uint(lx2.y) | __float_as_uint(ly2.y) | __float_as_uint(lz2.y) |
-                                            __float_as_uint(hx2.y) | __float_as_uint(hy2.y) | __float_as_uint(hz2.y);
-                        const float2 dX = __fadd2_rn(X, nmx), dY = __fadd2_rn(Y, nmy), dZ = __fadd2_rn(Z, nmz);
-                        // p2 = dx (q0 dx + q1 dy + q2 dz) + dy (q3 dy + q4 dz) + dz (q5 dz)
-                        float2 a = __ffma2_rn(Q0, dX, __ffma2_rn(Q1, dY, __fmul2_rn(Q2, dZ)));
-                        a = __fmul2_rn(dX, a);
-                        a = __ffma2_rn(dY, __ffma2_rn(Q3, dY, __fmul2_rn(Q4, dZ)), a);
-                        const float2 P2 = __ffma2_rn(dZ, __fmul2_rn(Q5, dZ), a);
-                        // window kLog2Floor <= p2 <= 0: p2 - floor and 0 - p2 (as -p2 + 0: +0 for p2 = -0)
-                        const float2 wl = __fadd2_rn(P2, make_float2(-kLog2Floor, -kLog2Floor));
-                        const float2 wh = __ffma2_rn(P2, M1, make_float2(0.0f, 0.0f));
-                        const bool c0 = (int)(b0 | __float_as_uint(wl.x) | __float_as_uint(wh.x)) >= 0;
-                        const bool c1 = (int)(b1 | __float_as_uint(wl.y) | __float_as_uint(wh.y)) >= 0;
-                        const float e0 = c0 ? ex2_approx(P2.x) : 0.f, e1 = c1 ? ex2_approx(P2.y) : 0.f;
-                        // E in two BF16 parts (~16 bits: e to 2^-16 relative); Psi keeps three
-                        const __nv_bfloat162 H = __floats2bfloat162_rn(e0, e1);
-                        const __nv_bfloat162 M = __floats2bfloat162_rn(e0 - __low2float(H), e1 - __high2float(H));
-                        hw[k >> 1] = *reinterpret_cast<const uint32_t*>(&H);
-                        mw[k >> 1] = *reinterpret_cast<const uint32_t*>(&M);
-                        if (COUNT) {
-                            const bool g0 = (rmask >> k) & 1u, g1 = (rmask >> (k + 1)) & 1u;
-                            ncand += ((g0 && (int)b0 >= 0) ? 1 : 0) + ((g1 && (int)b1 >= 0) ? 1 : 0);
-                            ncontrib += ((g0 && c0 && sm.rok[r]) ? 1 : 0) + ((g1 && c1 && sm.rok[r + 1]) ? 1 : 0);
-                            nlane += 64;
-                        }
+                for (int k = 0; k < 16; k += 2) {
+                    const int r = 16 * q + k;
+                    const float2 X = *reinterpret_cast<const float2*>(&sm.rx[r]);
+                    const float2 Y = *reinterpret_cast<const float2*>(&sm.ry[r]);
+                    const float2 Z = *reinterpret_cast<const float2*>(&sm.rz[r]);
+                    // rows of the chunk outside the group need no mask: their Psi rows are zero
+                    const float2 M1 = make_float2(-1.0f, -1.0f);
+                    const float2 lx2 = __fadd2_rn(X, NLX), ly2 = __fadd2_rn(Y, NLY), lz2 = __fadd2_rn(Z, NLZ);
+                    const float2 hx2 = __ffma2_rn(X, M1, HX), hy2 = __ffma2_rn(Y, M1, HY), hz2 = __ffma2_rn(Z, M1, HZ);
+                    const uint32_t b0 = __float_as_uint(lx2.x) | __float_as_uint(ly2.x) | __float_as_uint(lz2.x) |
+                                        __float_as_uint(hx2.x) | __float_as_uint(hy2.x) | __float_as_uint(hz2.x);
+                    const uint32_t b1 = __float_as_uint(lx2.y) | __float_as_uint(ly2.y) | __float_as_uint(lz2.y) |
+                                        __float_as_uint(hx2.y) | __float_as_uint(hy2.y) | __float_as_uint(hz2.y);
+                    const float2 dX = __fadd2_rn(X, nmx), dY = __fadd2_rn(Y, nmy), dZ = __fadd2_rn(Z, nmz);
+                    // p2 = dx (q0 dx + q1 dy + q2 dz) + dy (q3 dy + q4 dz) + dz (q5 dz)
+                    float2 a = __ffma2_rn(Q0, dX, __ffma2_rn(Q1, dY, __fmul2_rn(Q2, dZ)));
+                    a = __fmul2_rn(dX, a);
+                    a = __ffma2_rn(dY, __ffma2_rn(Q3, dY, __fmul2_rn(Q4, dZ)), a);
+                    const float2 P2 = __ffma2_rn(dZ, __fmul2_rn(Q5, dZ), a);
+                    // window kLog2Floor <= p2 <= 0: p2 - floor and 0 - p2 (as -p2 + 0: +0 for p2 = -0)
+                    const float2 wl = __fadd2_rn(P2, make_float2(-kLog2Floor, -kLog2Floor));
+                    const float2 wh = __ffma2_rn(P2, M1, make_float2(0.0f, 0.0f));
+                    const bool c0 = (int)(b0 | __float_as_uint(wl.x) | __float_as_uint(wh.x)) >= 0;
+                    const bool c1 = (int)(b1 | __float_as_uint(wl.y) | __float_as_uint(wh.y)) >= 0;
+                    const float e0 = c0 ? ex2_approx(P2.x) : 0.f, e1 = c1 ? ex2_approx(P2.y) : 0.f;
+                    // E in two BF16 parts (~16 bits: e to 2^-16 relative); Psi keeps three
+                    const __nv_bfloat162 H = __floats2bfloat162_rn(e0, e1);
+                    const __nv_bfloat162 M = __floats2bfloat162_rn(e0 - __low2float(H), e1 - __high2float(H));
+                    hw[k >> 1] = *reinterpret_cast<const uint32_t*>(&H);
+                    mw[k >> 1] = *reinterpret_cast<const uint32_t*>(&M);
+                    if (COUNT) {
+                        const bool g0 = (rmask >> k) & 1u, g1 = (rmask >> (k + 1)) & 1u;
+                        ncand += ((g0 && (int)b0 >= 0) ? 1 : 0) + ((g1 && (int)b1 >= 0) ? 1 : 0);
+                        ncontrib += ((g0 && c0 && sm.rok[r]) ? 1 : 0) + ((g1 && c1 && sm.rok[r + 1]) ? 1 : 0);
+                        nlane += 64;
                     }
                 }
                 tc_fence_after();

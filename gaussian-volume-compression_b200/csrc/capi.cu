@@ -200,7 +200,7 @@ void gvc_ctx_destroy(gvc_ctx* ctx) {
                           &L->onesweep};
         for (DevBuf* b : bufs) b->release();
     }
-    DevBuf* bufs[] = {&c->s_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->blk_desc_b, &c->blk_boxes_b, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
+    DevBuf* bufs[] = {&c->s_sorted, &c->fwd_sorted, &c->tile_boxes, &c->tile_keys, &c->tile_gdesc, &c->blk_desc, &c->blk_boxes, &c->blk_desc_b, &c->blk_boxes_b, &c->s_grad, &c->s_gyz, &c->s_ok, &c->grec, &c->gtmp,
                       &c->m_out_sorted, &c->knn_boxes, &c->ts_points, &c->ts_words, &c->ts_gt64, &c->scratch.gacc, &c->scratch.tmp_boxes, &c->scratch.tmp_out,
                       &c->clog, &c->cend};
     for (DevBuf* b : bufs) b->release();
@@ -324,6 +324,7 @@ int gvc_build_bvh(gvc_ctx* ctx, const float* samples, int64_t S, int debug, int 
     ctx->samples_ready = false;
     ctx->blk_b_ready = false;
     ctx->clog_ready = false;
+    ctx->fwd_sorted_ready = false;
     ctx->tiles_ready = false;        // the sample-group LBVH is built by its first user
     ctx->tile_groups_ready = false;  // so are the lane groups of the 32-sample tiles
     if (S > 0) {
@@ -380,6 +381,7 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
         GVC_CUDA(launch_fill_zero_outputs(S, out_cells, out_weights, st), "zero outputs");
         ctx->gauss_ready = false;
         ctx->clog_ready = false;
+        ctx->fwd_sorted_ready = false;
         return GVC_OK;
     }
     if (!means3D || !scales || !rotations || !values || !weights || !conics)
@@ -448,10 +450,25 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
                 ctx->cend.release();
             }
         }
+        // the FP32 forward also stores (out, W) in sorted order for the backward's sample records
+        if (ctx->eval_path == 0 && ctx->S > 0) {
+            if (ctx->fwd_sorted.ensure(sizeof(float2) * ctx->n_tiles * kTile) == cudaSuccess) {
+                ca.out_sorted = ctx->fwd_sorted.as<float2>();
+            } else {
+                (void)cudaGetLastError();
+                ctx->fwd_sorted.release();
+            }
+        }
         GVC_CUDA(launch_forward_cta(ca, ctx->eval_path == 1, st), "forward (CTA)");
         ctx->clog_ready = ca.clog != nullptr;
+        ctx->fwd_sorted_ready = ca.out_sorted != nullptr;
+        ctx->fwd_out_cells = out_cells;
+        ctx->fwd_out_weights = out_weights;
     }
-    if (ctx->eval_path == 2) ctx->clog_ready = false;
+    if (ctx->eval_path == 2) {
+        ctx->clog_ready = false;
+        ctx->fwd_sorted_ready = false;
+    }
     timer_end(ctx, st, tk);
     tm.mark();
     ctx->P = P;
@@ -505,8 +522,12 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
         GVC_CUDA(ctx->s_grad.ensure(sizeof(float4) * slots), "alloc s_grad");
         GVC_CUDA(ctx->s_gyz.ensure(sizeof(float) * slots), "alloc s_gyz");
         GVC_CUDA(ctx->s_ok.ensure(slots), "alloc s_ok");
-        GVC_CUDA(launch_sample_grads(slots, ctx->s_sorted.as<float4>(), out_cells, out_weights, dL_dout_cells,
-                                     dL_dout_weights, ctx->s_grad.as<float4>(), ctx->s_gyz.as<float>(),
+        // the forward's sorted copy of (out, W) when these are the arrays it wrote
+        const bool same_out = ctx->fwd_sorted_ready && have_order && out_cells == ctx->fwd_out_cells &&
+                              out_weights == ctx->fwd_out_weights;
+        GVC_CUDA(launch_sample_grads(slots, ctx->s_sorted.as<float4>(),
+                                     same_out ? ctx->fwd_sorted.as<float2>() : nullptr, out_cells, out_weights,
+                                     dL_dout_cells, dL_dout_weights, ctx->s_grad.as<float4>(), ctx->s_gyz.as<float>(),
                                      ctx->s_ok.as<uint8_t>(), st),
                  "sample grads");
         BwdArgs ba{};

@@ -26,19 +26,26 @@ __device__ __forceinline__ float ex2_apx(float x) {
 
 __device__ __forceinline__ float hp6(const Box6& b) { return (b.hx - b.lx) + (b.hy - b.ly) + (b.hz - b.lz); }
 
-// One warp per 128-row block; lane l holds rows 4l .. 4l + 3 (shuffles only, no block
-// barriers).  Box unions are min/max reductions, so the result does not depend on the
-// reduction order.
+// Order-preserving float <-> uint32 map: a < b as floats iff ord(a) < ord(b) as integers
+// (finite values and infinities; -0 orders below +0, which compare equal as floats).
+__device__ __forceinline__ uint32_t ford(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ordf(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// One warp per 128-row block; lane l holds rows 4l .. 4l + 3 (warp reductions only, no
+// block barriers).  Box unions are min/max reductions (one redux.sync each on the ordered
+// integers), so the result does not depend on the reduction order.
 __device__ __forceinline__ Box6 warp_reduce_box(Box6 b) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        b.lx = fminf(b.lx, __shfl_xor_sync(0xffffffffu, b.lx, off));
-        b.ly = fminf(b.ly, __shfl_xor_sync(0xffffffffu, b.ly, off));
-        b.lz = fminf(b.lz, __shfl_xor_sync(0xffffffffu, b.lz, off));
-        b.hx = fmaxf(b.hx, __shfl_xor_sync(0xffffffffu, b.hx, off));
-        b.hy = fmaxf(b.hy, __shfl_xor_sync(0xffffffffu, b.hy, off));
-        b.hz = fmaxf(b.hz, __shfl_xor_sync(0xffffffffu, b.hz, off));
-    }
+    b.lx = ordf(__reduce_min_sync(0xffffffffu, ford(b.lx)));
+    b.ly = ordf(__reduce_min_sync(0xffffffffu, ford(b.ly)));
+    b.lz = ordf(__reduce_min_sync(0xffffffffu, ford(b.lz)));
+    b.hx = ordf(__reduce_max_sync(0xffffffffu, ford(b.hx)));
+    b.hy = ordf(__reduce_max_sync(0xffffffffu, ford(b.hy)));
+    b.hz = ordf(__reduce_max_sync(0xffffffffu, ford(b.hz)));
     return b;
 }
 
@@ -80,9 +87,7 @@ __device__ int rows_split(int a, int b, const Box6& B, Box6& B1, Box6& B2, const
         const int row = 4 * lane + k;
         if (row >= a && row < b && ((key[k] >> bit) & 1u)) first = min(first, row);
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, off));
-    const int m = first;
+    const int m = (int)__reduce_min_sync(0xffffffffu, (unsigned)first);
     B1 = rows_box(a, m, x, y, z);
     B2 = rows_box(m, b, x, y, z);
     return fmaxf(hp6(B1), hp6(B2)) <= ratio * hp6(B) ? m : -1;
@@ -364,7 +369,8 @@ __global__ void __launch_bounds__(kConsumerWarps * 32 + 32, kCtaMinBlocks)
     k_forward_cta(const float4* __restrict__ s_sorted, int64_t S, const uint2* __restrict__ bdesc,
                   const float4* __restrict__ bboxes, const BvhNode* __restrict__ nodes, int64_t n_internal,
                   const GaussRec* __restrict__ recs, float* __restrict__ out_cells, float* __restrict__ out_weights,
-                  int32_t* __restrict__ clog, int32_t* __restrict__ cend, int* status, unsigned long long* stats) {
+                  float2* __restrict__ out_sorted, int32_t* __restrict__ clog, int32_t* __restrict__ cend, int* status,
+                  unsigned long long* stats) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CtaSmem& sm = *reinterpret_cast<CtaSmem*>(smem_raw);
     constexpr int RPT = kRowsPerThread;
@@ -529,6 +535,9 @@ __global__ void __launch_bounds__(kConsumerWarps * 32 + 32, kCtaMinBlocks)
                 }
                 out_cells[orig[k]] = o;
                 out_weights[orig[k]] = ww;
+                // the same pair in sorted order (coalesced), so that the backward's sample
+                // records need not gather them back
+                if (out_sorted) out_sorted[blk * kBlockRows + (w * RPT + k) * 32 + lane] = make_float2(o, ww);
             }
         }
         if (COUNT) {
@@ -566,8 +575,8 @@ static cudaError_t launch_cta_impl(const CtaArgs& a, cudaStream_t st) {
         cudaFuncSetAttribute(k_forward_cta<COUNT, STACKLESS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_forward_cta<COUNT, STACKLESS><<<nblk128(a.S), kConsumerWarps * 32 + 32, smem, st>>>(
-        a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.n_internal, a.recs, a.out_cells, a.out_weights, a.clog,
-        a.cend, a.status, a.stats);
+        a.s_sorted, a.S, a.bdesc, a.bboxes, a.gnodes, a.n_internal, a.recs, a.out_cells, a.out_weights,
+        a.out_sorted, a.clog, a.cend, a.status, a.stats);
     gvc::note_launch();
     return cudaGetLastError();
 }

@@ -118,6 +118,12 @@ struct gvc_ctx {
     // candidate log of the last block-group forward (for the tensor-core backward)
     gvc::DevBuf clog, cend;
     bool clog_ready = false;
+    // (out, W) per sorted slot as the last FP32 block-group forward wrote them, and the
+    // output arrays it wrote them to (the backward uses the copy for those arrays only)
+    gvc::DevBuf fwd_sorted;
+    const float* fwd_out_cells = nullptr;
+    const float* fwd_out_weights = nullptr;
+    bool fwd_sorted_ready = false;
     gvc::DevBuf s_sorted;   // [n_tiles*32] float4 (x, y, z, bits of caller index or -1)
     gvc::DevBuf tile_boxes; // [n_tiles * kGroups] group boxes, 2 x float4 (empty for unused slots)
     gvc::DevBuf tile_keys;  // [n_tiles * kGroups] uint32 Morton key of each group's first sample

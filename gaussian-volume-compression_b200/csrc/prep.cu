@@ -293,7 +293,10 @@ __global__ void __launch_bounds__(256) k_sample_tiles(int64_t S, int64_t n_tiles
 // -dL/dout * out / W + dL/dW (backward.cu:252-298 folds the same factors per pair), and
 // ok = W > 0.01.  Samples below the cutoff get gx = gyz = 0, so their pairs add exactly
 // nothing; tile padding gets finite coordinates (0) and zero gradients for the same reason.
+// With out_sorted (the forward's (out, W) per sorted slot) only dL/dout and dL/dW are
+// gathered from the caller's order.
 __global__ void __launch_bounds__(256) k_sample_grads(int64_t n_slots, const float4* __restrict__ s_sorted,
+                                                      const float2* __restrict__ out_sorted,
                                                       const float* __restrict__ out_cells,
                                                       const float* __restrict__ out_weights,
                                                       const float* __restrict__ gout, const float* __restrict__ gw,
@@ -307,11 +310,12 @@ __global__ void __launch_bounds__(256) k_sample_grads(int64_t n_slots, const flo
     uint8_t ok = 0;
     float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
     if (o >= 0) {
-        const float W = out_weights[o];
+        const float2 ow = out_sorted ? out_sorted[i] : make_float2(0.f, out_weights[o]);
+        const float W = ow.y;
         if (W > kWeightCutoff) {
             const float g = gout[o];
             gx = g / W;
-            gyz = -(g * out_cells[o]) / W + gw[o];
+            gyz = -(g * (out_sorted ? ow.x : out_cells[o])) / W + gw[o];
             ok = 1;
         }
         r = make_float4(sp.x, sp.y, sp.z, gx);
@@ -347,12 +351,12 @@ cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples
     return cudaGetLastError();
 }
 
-cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float* out_cells,
-                                const float* out_weights, const float* gout, const float* gw, float4* s_grad,
-                                float* s_gyz, uint8_t* s_ok, cudaStream_t st) {
+cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float2* out_sorted,
+                                const float* out_cells, const float* out_weights, const float* gout, const float* gw,
+                                float4* s_grad, float* s_gyz, uint8_t* s_ok, cudaStream_t st) {
     if (n_slots <= 0) return cudaSuccess;
-    k_sample_grads<<<nb256(n_slots), 256, 0, st>>>(n_slots, s_sorted, out_cells, out_weights, gout, gw, s_grad,
-                                                   s_gyz, s_ok); gvc::note_launch();
+    k_sample_grads<<<nb256(n_slots), 256, 0, st>>>(n_slots, s_sorted, out_sorted, out_cells, out_weights, gout, gw,
+                                                   s_grad, s_gyz, s_ok); gvc::note_launch();
     return cudaGetLastError();
 }
 

@@ -96,6 +96,7 @@ struct CtaArgs {
     const GaussRec* recs;
     float* out_cells;
     float* out_weights;
+    float2* out_sorted;    // (out, W) per sorted slot, read by the backward's sample records; or null
     int* status;
     unsigned long long* stats;
     bool count;
@@ -135,9 +136,11 @@ cudaError_t launch_gather_recs(int64_t P, const int32_t* perm, const float* mean
 cudaError_t launch_sample_tiles(int64_t S, int64_t n_tiles, const float* samples, const int32_t* perm,
                                 const uint32_t* skeys, float4* s_sorted, float4* group_boxes, uint32_t* group_keys,
                                 uint32_t* gdesc, bool with_groups, cudaStream_t st);
-cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float* out_cells,
-                                const float* out_weights, const float* gout, const float* gw, float4* s_grad,
-                                float* s_gyz, uint8_t* s_ok, cudaStream_t st);
+// out_sorted: the forward's (out, W) per sorted slot when the caller's out_cells /
+// out_weights are that forward's outputs (else null: they are gathered).
+cudaError_t launch_sample_grads(int64_t n_slots, const float4* s_sorted, const float2* out_sorted,
+                                const float* out_cells, const float* out_weights, const float* gout, const float* gw,
+                                float4* s_grad, float* s_gyz, uint8_t* s_ok, cudaStream_t st);
 cudaError_t launch_fill_zero_outputs(int64_t S, float* out_cells, float* out_weights, cudaStream_t st);
 
 // mesh.cu

@@ -239,6 +239,36 @@ def test_deterministic_backward_is_bitwise_reproducible(cuda, small_case):
         np.testing.assert_array_equal(x, y)
 
 
+def test_backward_sorted_outputs_match_gathered(cuda, small_case):
+    """The FP32 forward also keeps (out, W) in sorted order for the backward's per-sample
+    records; the backward reads that copy when it is handed the forward's own output
+    arrays and gathers them from the caller's order otherwise (here: copies of them).
+    Both give the same gradients bit for bit (deterministic backward, nonzero dL/dW)."""
+    from bvh_diff_gaussian_rasterization import _C
+    means, scales, rots, values, weights, samples = small_case
+    S = samples.shape[0]
+    rng = np.random.default_rng(11)
+    gout = T(rng.normal(size=S).astype(np.float32), cuda)
+    gw = T(rng.normal(size=S).astype(np.float32), cuda)
+    out, outw, conics = run_forward(cuda, *small_case)
+
+    def bwd(o, ow):
+        return _C.rasterize_gaussians_backward(T(means, cuda), T(scales, cuda), T(rots, cuda), conics,
+                                               T(values, cuda), T(weights, cuda), o, ow, 1.0, 0, 0, 0, 1, 1, 1,
+                                               -1.0, gout, gw, False, False)
+
+    _C.set_backward_mode("deterministic")
+    try:
+        a = bwd(out, outw)
+        b = bwd(out.clone(), outw.clone())
+        _C.check_status()
+    finally:
+        _C.set_backward_mode("auto")
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    assert any(bool(x.abs().max() > 0) for x in a)
+
+
 def _raw_params(kind):
     """Pre-activation parameters: 'small' (512 Gaussians on a 24^3 grid) or 'config1'
     (4096 Gaussians, means U[0,1]^3, log-scales N(log 0.02, 0.3), random quaternions,
