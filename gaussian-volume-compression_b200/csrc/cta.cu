@@ -68,14 +68,9 @@ __device__ __forceinline__ Box6 rows_box(int a, int b, const float (&x)[4], cons
     return warp_reduce_box(r);
 }
 
-// Split row of [a, b) or -1 (warp-uniform): at the first Morton bit where the range's
-// first and last keys differ, taken when both halves' boxes have at most half the
-// half-perimeter of the whole.  B is the box of [a, b); on a split B1 and B2 receive the
-// boxes of the two halves (box unions are exact, so a box computed once for a range is
-// the box of that range wherever it is used).
-__device__ int rows_split(int a, int b, const Box6& B, Box6& B1, Box6& B2, const uint32_t* keys,
-                          const uint32_t (&key)[4], const float (&x)[4], const float (&y)[4], const float (&z)[4],
-                          float ratio) {
+// Candidate split row of [a, b) or -1 (warp-uniform): the first row at the first Morton
+// bit where the range's first and last keys differ.
+__device__ __forceinline__ int rows_split_row(int a, int b, const uint32_t* keys, const uint32_t (&key)[4]) {
     if (b - a < 2) return -1;
     const uint32_t ka = keys[a], kb = keys[b - 1];
     if (ka == kb) return -1;
@@ -87,10 +82,7 @@ __device__ int rows_split(int a, int b, const Box6& B, Box6& B1, Box6& B2, const
         const int row = 4 * lane + k;
         if (row >= a && row < b && ((key[k] >> bit) & 1u)) first = min(first, row);
     }
-    const int m = (int)__reduce_min_sync(0xffffffffu, (unsigned)first);
-    B1 = rows_box(a, m, x, y, z);
-    B2 = rows_box(m, b, x, y, z);
-    return fmaxf(hp6(B1), hp6(B2)) <= ratio * hp6(B) ? m : -1;
+    return (int)__reduce_min_sync(0xffffffffu, (unsigned)first);
 }
 
 constexpr int kBlocksPerCta = 8;  // 128-row blocks (warps) per CTA of k_sample_blocks
@@ -101,57 +93,107 @@ __device__ __forceinline__ Box6 shfl_box(const Box6& b, int src) {
                 __shfl_sync(0xffffffffu, b.hy, src), __shfl_sync(0xffffffffu, b.hz, src)};
 }
 
-// Splits the block's valid rows [0, nvalid) (box B0) three times (every range of a level
-// in order, at most 8 groups) with `ratio` and writes bdesc[blk] = (starts of groups
-// 1..7 as bytes, 128 if unused; byte 7 = group count) and bboxes[blk * 8 + g] = (lo, hi)
-// of group g (empty box if unused).  The box of range i of a level is held by lane i.
-__device__ __forceinline__ void block_split_store(int64_t blk, int nvalid, const Box6& B0, const uint32_t* keys,
-                                                  const uint32_t (&key)[4], const float (&x)[4],
-                                                  const float (&y)[4], const float (&z)[4], float ratio,
-                                                  uint2* __restrict__ bdesc, float4* __restrict__ bboxes) {
+// Split tree of one block's valid rows [0, nvalid): node 1 is the block, nodes 2i and
+// 2i + 1 are the halves of node i, three levels (at most 8 groups).  A range splits at its
+// Morton split row when both halves' boxes have at most `ratio` of its half-perimeter.
+// A split taken with some ratio is taken with every larger one at the same row, so the tree
+// is built once with the larger of the two ratios, recording each node's two half-perimeter
+// figures, and each ratio's groups are the leaves of the subtree whose splits pass its own
+// test (the same float comparison as a tree built with that ratio alone).  Box unions are
+// exact, so each node's box is computed once.  Lane i holds node i's fields.
+struct SplitTree {
+    Box6 box;    // box of node i
+    int a, b;    // rows [a, b) of node i
+    float h12;   // max(hp(half 1), hp(half 2)), +inf where node i has no split row
+    float h;     // hp(node i)
+};
+
+__device__ __forceinline__ SplitTree split_tree_build(int nvalid, float rmax, const uint32_t* keys,
+                                                      const uint32_t (&key)[4], const float (&x)[4],
+                                                      const float (&y)[4], const float (&z)[4]) {
     const int lane = threadIdx.x & 31;
-    int ra[kBlockGroups], rb[kBlockGroups];
-    int nr = 1;
-    ra[0] = 0;
-    rb[0] = nvalid;
-    Box6 lb = B0;  // lane i: box of range i
-    for (int depth = 0; depth < 3; depth++) {
-        int na[kBlockGroups], nbb[kBlockGroups];
-        Box6 nlb = lb;
-        int nn = 0;
-        for (int i = 0; i < nr; i++) {
-            const Box6 Bi = shfl_box(lb, i);
-            Box6 B1, B2;
-            const int m = rows_split(ra[i], rb[i], Bi, B1, B2, keys, key, x, y, z, ratio);
-            if (m >= 0) {
-                if (lane == nn) nlb = B1;
-                na[nn] = ra[i];
-                nbb[nn++] = m;
-                if (lane == nn) nlb = B2;
-                na[nn] = m;
-                nbb[nn++] = rb[i];
-            } else {
-                if (lane == nn) nlb = Bi;
-                na[nn] = ra[i];
-                nbb[nn++] = rb[i];
+    SplitTree T;
+    T.box = rows_box(0, nvalid, x, y, z);
+    T.a = 0;
+    T.b = nvalid;
+    T.h12 = INFINITY;
+    T.h = 0.f;
+    bool ex[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) ex[i] = i == 1;
+#pragma unroll
+    for (int i = 1; i < 8; i++) {
+        if (!ex[i]) continue;  // warp-uniform
+        const int ai = __shfl_sync(0xffffffffu, T.a, i), bi = __shfl_sync(0xffffffffu, T.b, i);
+        const int m = rows_split_row(ai, bi, keys, key);
+        if (m < 0) continue;
+        const Box6 B = shfl_box(T.box, i);
+        const Box6 B1 = rows_box(ai, m, x, y, z);
+        const Box6 B2 = rows_box(m, bi, x, y, z);
+        const float h12 = fmaxf(hp6(B1), hp6(B2)), h = hp6(B);
+        if (lane == i) {
+            T.h12 = h12;
+            T.h = h;
+        }
+        if (h12 <= rmax * h) {
+            ex[2 * i] = ex[2 * i + 1] = true;
+            if (lane == 2 * i) {
+                T.box = B1;
+                T.a = ai;
+                T.b = m;
+            }
+            if (lane == 2 * i + 1) {
+                T.box = B2;
+                T.a = m;
+                T.b = bi;
             }
         }
-        for (int i = 0; i < nn; i++) {
-            ra[i] = na[i];
-            rb[i] = nbb[i];
+    }
+    return T;
+}
+
+// Groups of `ratio` from the tree: bdesc[blk] = (starts of groups 1..7 as bytes, 128 if
+// unused; byte 7 = group count), bboxes[blk * 8 + g] = (lo, hi) of group g (empty box if
+// unused).
+__device__ __forceinline__ void split_tree_store(const SplitTree& T, int64_t blk, float ratio,
+                                                 uint2* __restrict__ bdesc, float4* __restrict__ bboxes) {
+    const int lane = threadIdx.x & 31;
+    const bool splits = T.h12 <= ratio * T.h;  // lane i: node i splits with this ratio
+    const uint32_t sm = __ballot_sync(0xffffffffu, splits);
+    int ids[kBlockGroups];
+    int nr = 1;
+    ids[0] = 1;
+    for (int depth = 0; depth < 3; depth++) {
+        int nid[kBlockGroups];
+        int nn = 0;
+        for (int k = 0; k < nr; k++) {
+            const int i = ids[k];
+            if ((sm >> i) & 1u) {
+                nid[nn++] = 2 * i;
+                nid[nn++] = 2 * i + 1;
+            } else {
+                nid[nn++] = i;
+            }
         }
-        lb = nlb;
+        for (int k = 0; k < nn; k++) ids[k] = nid[k];
         nr = nn;
     }
+    const int mine = lane < nr ? ids[lane] : 0;
+    const Box6 G = shfl_box(T.box, mine);
+    const int start = __shfl_sync(0xffffffffu, T.a, mine);
     if (lane < kBlockGroups) {
         Box6 B{INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-        if (lane < nr) B = lb;
+        if (lane < nr) B = G;
         bboxes[2 * (blk * kBlockGroups + lane)] = make_float4(B.lx, B.ly, B.lz, 0.f);
         bboxes[2 * (blk * kBlockGroups + lane) + 1] = make_float4(B.hx, B.hy, B.hz, 0.f);
     }
+    uint32_t starts[kBlockGroups];
+#pragma unroll
+    for (int g = 0; g < kBlockGroups; g++) {
+        const int sg = __shfl_sync(0xffffffffu, start, g);
+        starts[g] = g < nr ? (uint32_t)sg : (uint32_t)kBlockRows;
+    }
     if (lane == 0) {
-        uint32_t starts[kBlockGroups];
-        for (int g = 0; g < kBlockGroups; g++) starts[g] = g < nr ? (uint32_t)ra[g] : (uint32_t)kBlockRows;
         uint2 d;
         d.x = starts[1] | (starts[2] << 8) | (starts[3] << 16) | (starts[4] << 24);
         d.y = starts[5] | (starts[6] << 8) | (starts[7] << 16) | ((uint32_t)nr << 24);
@@ -191,9 +233,9 @@ __global__ void __launch_bounds__(32 * kBlocksPerCta) k_sample_blocks(const floa
     __syncwarp();
     const int64_t rem = S - blk * kBlockRows;
     const int nvalid = rem < kBlockRows ? (int)rem : kBlockRows;
-    const Box6 B0 = rows_box(0, nvalid, x, y, z);
-    block_split_store(blk, nvalid, B0, keys, key, x, y, z, ratio, bdesc, bboxes);
-    if (bdesc2) block_split_store(blk, nvalid, B0, keys, key, x, y, z, ratio2, bdesc2, bboxes2);
+    const SplitTree T = split_tree_build(nvalid, bdesc2 ? fmaxf(ratio, ratio2) : ratio, keys, key, x, y, z);
+    split_tree_store(T, blk, ratio, bdesc, bboxes);
+    if (bdesc2) split_tree_store(T, blk, ratio2, bdesc2, bboxes2);
 }
 
 // ---------------------------------------------------------------------------------------

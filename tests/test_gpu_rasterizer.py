@@ -80,8 +80,11 @@ def gpu_lbvh(ctx, dev, boxes):
             right.cpu().numpy()[:n - 1], nb.cpu().numpy().reshape(-1, 6)[:n - 1])
 
 
+# 4096 keys per radix-sort tile: 300k keys are one wave of tiles; 2.5M keys (611 tiles) are
+# more than the 592 blocks resident at once, so later tiles look back over finished ones
 @pytest.mark.parametrize("n,kind", [(1, "rand"), (2, "rand"), (3, "rand"), (33, "rand"), (1000, "rand"),
-                                    (4097, "dup"), (20000, "same"), (300000, "rand"), (300000, "dup")])
+                                    (4097, "dup"), (20000, "same"), (300000, "rand"), (300000, "dup"),
+                                    (2500000, "dup")])
 def test_lbvh_bit_exact(ctx, cuda, orc, n, kind):
     rng = np.random.default_rng(n)
     c = rng.random((n, 3)).astype(np.float32)
@@ -97,12 +100,12 @@ def test_lbvh_bit_exact(ctx, cuda, orc, n, kind):
         np.testing.assert_array_equal(a, b, err_msg=name)
 
 
-def test_sample_order_bit_exact(cuda, orc):
+@pytest.mark.parametrize("S", [100003, 5000001])
+def test_sample_order_bit_exact(cuda, orc, S):
     from bvh_diff_gaussian_rasterization import _C
     rng = np.random.default_rng(11)
-    S = 100003
     pts = rng.random((S, 3)).astype(np.float32)
-    pts[:1000] = np.round(pts[:1000] * 4) / 4  # duplicate keys
+    pts[:S // 100] = np.round(pts[:S // 100] * 4) / 4  # duplicate keys
     _C.build_bvh(T(pts, cuda), False, False)
     perm = torch.empty(S, dtype=torch.int32, device=cuda)
     keys = torch.empty(S, dtype=torch.int32, device=cuda)
