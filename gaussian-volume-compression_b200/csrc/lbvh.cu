@@ -319,7 +319,7 @@ constexpr uint32_t kOsAggregate = 1u << 30;
 constexpr uint32_t kOsInclusive = 2u << 30;
 constexpr uint32_t kOsCount = (1u << 30) - 1u;
 constexpr long long kOsSpinCycles = 200000000LL;  // ~0.1 s at 2 GHz
-constexpr int kOsWindow = 16;                    // look-back words read per round trip
+constexpr int kOsWindow = 16;                    // look-back words loaded together
 
 __device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t* p) {
     uint32_t v;
@@ -463,8 +463,8 @@ __global__ void __launch_bounds__(256, 4) k_os_scatter(const uint32_t* __restric
         }
     }
     // look back for the count of digit d in all tiles before this one, kOsWindow words
-    // per round trip: aggregates are added until an inclusive prefix is met; a tile not
-    // ready yet stops the round (the words before it are kept) and is read again
+    // loaded together: aggregates are added until an inclusive prefix is met; a tile not
+    // ready yet ends this window (the words before it are kept) and is read again
     if (tile > 0) {
         uint32_t excl = 0;
         int64_t k = tile - 1;  // nearest tile not accounted for yet
