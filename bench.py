@@ -68,7 +68,7 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 TENSOR_PIPE_ACTIVE = {"k_backward_cta": 0.358, "k_forward_tc": 0.189}
 MEASURED_TRAFFIC = {("large", "k_backward_cta"): 1.291e9 + 0.142e9,
                     ("large", "k_backward_gauss"): 1.475e9 + 0.125e9,
-                    ("large", "k_forward_cta"): 1.566e9 + 1.640e9}
+                    ("large", "k_forward_cta"): 1.585e9 + 1.774e9}
 
 
 def parse():
