@@ -382,6 +382,7 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
         ctx->gauss_ready = false;
         ctx->clog_ready = false;
         ctx->fwd_sorted_ready = false;
+        ctx->fwd_recs_ready = false;
         return GVC_OK;
     }
     if (!means3D || !scales || !rotations || !values || !weights || !conics)
@@ -473,6 +474,14 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
     tm.mark();
     ctx->P = P;
     ctx->gauss_ready = true;
+    ctx->fwd_means = means3D;
+    ctx->fwd_scales = scales;
+    ctx->fwd_rots = rotations;
+    ctx->fwd_values = values;
+    ctx->fwd_weights = weights;
+    ctx->fwd_conics = conics;
+    ctx->fwd_scale_mod = scale_modifier;
+    ctx->fwd_recs_ready = true;
     if (debug) {
         int rc = debug_check(ctx, st);
         printf("Preprocess time: %g ms\nBVH time: %g ms\nRender time: %g ms\n", tm.ms(0, 1), tm.ms(1, 2),
@@ -505,10 +514,20 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
     Scratch* sc = scratch_of(ctx);
     DebugTimer tm(debug != 0, st);
     tm.mark();
+    // Handed the very arrays of the last forward (and its conics), the forward's AABBs and
+    // LBVH-ordered records still hold; otherwise both are rebuilt here (and no longer
+    // describe that forward).
+    const bool same_gauss = ctx->fwd_recs_ready && ctx->gauss_ready && ctx->P == P && means3D == ctx->fwd_means &&
+                            scales == ctx->fwd_scales && rotations == ctx->fwd_rots && values == ctx->fwd_values &&
+                            weights == ctx->fwd_weights && conics == ctx->fwd_conics &&
+                            scale_modifier == ctx->fwd_scale_mod;
     GVC_CUDA(ctx->gtmp.ensure(sizeof(float4) * 2 * P), "alloc boxes");
     float4* boxes = ctx->gtmp.as<float4>();
-    GVC_CUDA(launch_preprocess(P, means3D, scales, rotations, weights, scale_modifier, nullptr, boxes, st),
-             "preprocess");
+    if (!same_gauss) {
+        ctx->fwd_recs_ready = false;
+        GVC_CUDA(launch_preprocess(P, means3D, scales, rotations, weights, scale_modifier, nullptr, boxes, st),
+                 "preprocess");
+    }
     GVC_CUDA(sc->gacc.ensure(sizeof(float) * 16 * P), "alloc gacc");
     float* gacc = sc->gacc.as<float>();
     // mode 3, or the tensor-core path in auto mode: reduction over samples on tcgen05
@@ -557,10 +576,12 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
         tm.mark();
         if (tc_bwd) {
             if (!have_order) GVC_CUDA(lbvh_build_boxes(ctx->gbvh, P, boxes, st), "Gaussian LBVH");
-            GVC_CUDA(ctx->grec.ensure(sizeof(GaussRec) * P), "alloc records");
-            GVC_CUDA(launch_gather_recs(P, ctx->gbvh.perm.as<int32_t>(), means3D, values, weights, conics, boxes,
-                                        ctx->grec.as<GaussRec>(), st),
-                     "gather records");
+            if (!same_gauss) {
+                GVC_CUDA(ctx->grec.ensure(sizeof(GaussRec) * P), "alloc records");
+                GVC_CUDA(launch_gather_recs(P, ctx->gbvh.perm.as<int32_t>(), means3D, values, weights, conics,
+                                            boxes, ctx->grec.as<GaussRec>(), st),
+                         "gather records");
+            }
             GVC_CUDA(cudaMemsetAsync(gacc, 0, sizeof(float) * 16 * P, st), "zero gacc");
             ba.gorder = nullptr;
             ba.gperm = ctx->gbvh.perm.as<int32_t>();
@@ -592,10 +613,12 @@ int gvc_rasterize_gaussians_backward(gvc_ctx* ctx, int64_t P, const float* means
             timer_end(ctx, st, tk);
         } else if (atomic_mode) {
             if (!have_order) GVC_CUDA(lbvh_build_boxes(ctx->gbvh, P, boxes, st), "Gaussian LBVH");
-            GVC_CUDA(ctx->grec.ensure(sizeof(GaussRec) * P), "alloc records");
-            GVC_CUDA(launch_gather_recs(P, ctx->gbvh.perm.as<int32_t>(), means3D, values, weights, conics, boxes,
-                                        ctx->grec.as<GaussRec>(), st),
-                     "gather records");
+            if (!same_gauss) {
+                GVC_CUDA(ctx->grec.ensure(sizeof(GaussRec) * P), "alloc records");
+                GVC_CUDA(launch_gather_recs(P, ctx->gbvh.perm.as<int32_t>(), means3D, values, weights, conics,
+                                            boxes, ctx->grec.as<GaussRec>(), st),
+                         "gather records");
+            }
             GVC_CUDA(cudaMemsetAsync(gacc, 0, sizeof(float) * 16 * P, st), "zero gacc");
             ba.gorder = nullptr;
             ba.gperm = ctx->gbvh.perm.as<int32_t>();

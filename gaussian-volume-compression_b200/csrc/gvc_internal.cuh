@@ -124,6 +124,16 @@ struct gvc_ctx {
     const float* fwd_out_cells = nullptr;
     const float* fwd_out_weights = nullptr;
     bool fwd_sorted_ready = false;
+    // the Gaussian arrays of the last forward: its AABBs (gtmp) and records (grec) are
+    // reused by a backward handed the same arrays
+    const float* fwd_means = nullptr;
+    const float* fwd_scales = nullptr;
+    const float* fwd_rots = nullptr;
+    const float* fwd_values = nullptr;
+    const float* fwd_weights = nullptr;
+    const float* fwd_conics = nullptr;
+    float fwd_scale_mod = 0.f;
+    bool fwd_recs_ready = false;
     gvc::DevBuf s_sorted;   // [n_tiles*32] float4 (x, y, z, bits of caller index or -1)
     gvc::DevBuf tile_boxes; // [n_tiles * kGroups] group boxes, 2 x float4 (empty for unused slots)
     gvc::DevBuf tile_keys;  // [n_tiles * kGroups] uint32 Morton key of each group's first sample
