@@ -387,6 +387,9 @@ int gvc_rasterize_gaussians(gvc_ctx* ctx, int64_t P, const float* means3D, const
     }
     if (!means3D || !scales || !rotations || !values || !weights || !conics)
         return fail(ctx, GVC_ERR_ARG, "null Gaussian parameter pointer");
+    // this call rewrites the AABBs, records and sorted outputs: valid again only once it ends
+    ctx->fwd_recs_ready = false;
+    ctx->fwd_sorted_ready = false;
     DebugTimer tm(debug != 0, st);
     if (ctx->count_pairs) GVC_CUDA(cudaMemsetAsync(ctx->d_stats, 0, sizeof(unsigned long long) * 16, st), "stats");
     tm.mark();
