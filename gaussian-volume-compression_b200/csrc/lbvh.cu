@@ -607,6 +607,12 @@ cudaError_t radix_sort_words(Lbvh& L, int64_t n, const uint32_t* const* words, c
     int32_t* vin = nullptr;  // identity before the first pass
     int32_t* vout = L.perm_alt.as<int32_t>();
     const unsigned gb = (unsigned)((n + 255) / 256);
+    // one kernel per pass (as radix_sort_pairs) where a status word takes the look-back's report
+    const bool os = L.status && n <= (int64_t)kOsCount;
+    const size_t os_head = sizeof(uint32_t) * (4 * 256 + 64);
+    const size_t os_look = sizeof(uint32_t) * 256 * (size_t)nb;
+    if (os && (e = L.onesweep.ensure(os_head + 4 * os_look)) != cudaSuccess) return e;
+    uint32_t* ghist = os ? L.onesweep.as<uint32_t>() : nullptr;
     for (int w = 0; w < nwords; w++) {
         const int passes = (bits[w] + 7) / 8;
         if (passes <= 0) continue;
@@ -617,10 +623,21 @@ cudaError_t radix_sort_words(Lbvh& L, int64_t n, const uint32_t* const* words, c
                    cudaSuccess) {
             return e;
         }
+        if (os) {
+            if ((e = cudaMemsetAsync(ghist, 0, os_head + (size_t)passes * os_look, st)) != cudaSuccess) return e;
+            k_os_hist<<<(unsigned)(nb < 148 * 4 ? nb : 148 * 4), 256, 0, st>>>(kin, n, ghist); gvc::note_launch();
+        }
         for (int pass = 0; pass < passes; pass++) {
-            k_rs_hist<<<nb, 256, 0, st>>>(kin, n, nb, pass, hist); gvc::note_launch();
-            k_rs_scan<<<256, 1024, 0, st>>>(hist, nb, totals); gvc::note_launch();
-            k_rs_scatter<<<nb, 256, 0, st>>>(kin, vin, kout, vout, n, nb, pass, hist, totals); gvc::note_launch();
+            if (os) {
+                k_os_scatter<<<(unsigned)nb, 256, 0, st>>>(kin, vin, kout, vout, n, pass, ghist,
+                                                           ghist + os_head / sizeof(uint32_t) +
+                                                               (size_t)pass * 256 * (size_t)nb,
+                                                           ghist + 4 * 256 + pass, L.status); gvc::note_launch();
+            } else {
+                k_rs_hist<<<nb, 256, 0, st>>>(kin, n, nb, pass, hist); gvc::note_launch();
+                k_rs_scan<<<256, 1024, 0, st>>>(hist, nb, totals); gvc::note_launch();
+                k_rs_scatter<<<nb, 256, 0, st>>>(kin, vin, kout, vout, n, nb, pass, hist, totals); gvc::note_launch();
+            }
             uint32_t* tk = kin;
             kin = kout;
             kout = tk;
