@@ -723,10 +723,11 @@ __global__ void __launch_bounds__(256) k_refit(int n, const int32_t* __restrict_
     if (i >= n) return;
     int node = parent[n - 1 + i];
     while (node >= 0) {
-        __threadfence();
-        uint32_t old = atomicAdd(&flags[node], 1u);
+        // acquire-release at GPU scope: the first child's box (stored before its arrival)
+        // is visible to the second arriver, which goes on with the node
+        uint32_t old;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(flags + node) : "memory");
         if (old == 0) return;
-        __threadfence();
         float4 alo, ahi, blo, bhi;
         load_child_box(left[node], leaf_boxes, node_boxes, alo, ahi);
         load_child_box(right[node], leaf_boxes, node_boxes, blo, bhi);
