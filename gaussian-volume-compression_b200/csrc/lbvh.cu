@@ -1,6 +1,7 @@
 // lbvh.cu -- on-device LBVH construction: 30-bit Morton keys, stable LSD radix sort
-// (8-bit digits, per-pass block histograms, warp-aggregated stable ranking),
-// Karras 2012 hierarchy, atomic bottom-up refit and node packing.
+// (8-bit digits, warp-aggregated stable ranking; one kernel per pass with decoupled
+// look-back, or per-pass block histograms + scan + scatter where no status word is
+// given), Karras 2012 hierarchy, atomic bottom-up refit and node packing.
 //
 // Replaces cuBQL::cuda::radixBuilder as called from
 // diff-gaussian-rasterization/cuda_rasterizer/rasterizer_impl.cu:78-83 (Gaussian AABBs)
