@@ -37,3 +37,22 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     with pytest.raises(RuntimeError, match="libgvc.so not found"):
         gvc_native.lib()
 
+
+def _enum_values(pattern):
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    return {m.group(1): int(m.group(2)) for m in re.finditer(r"\b(%s)\s*=\s*(\d+)" % pattern, src)}
+
+
+def test_status_and_option_codes_match_header():
+    """gvc_status and the option codes of include/gvc.h against the ctypes binding."""
+    import gvc_native
+    status = _enum_values(r"GVC_OK|GVC_ERR_[A-Z_]+")
+    assert {v: k for k, v in status.items()} == gvc_native.STATUS_NAMES
+    assert status["GVC_ERR_TRAVERSAL"] == gvc_native.GVC_ERR_TRAVERSAL
+    assert status["GVC_ERR_TIMEOUT"] == gvc_native.GVC_ERR_TIMEOUT
+    opts = _enum_values(r"GVC_OPT_[A-Z_]+")
+    py = {"GVC_OPT_COV_GRAD": gvc_native.OPT_COV_GRAD, "GVC_OPT_BWD_MODE": gvc_native.OPT_BWD_MODE,
+          "GVC_OPT_EVAL_PATH": gvc_native.OPT_EVAL_PATH, "GVC_OPT_COUNT_PAIRS": gvc_native.OPT_COUNT_PAIRS,
+          "GVC_OPT_TIME_KERNELS": gvc_native.OPT_TIME_KERNELS, "GVC_OPT_TRAVERSAL": gvc_native.OPT_TRAVERSAL,
+          "GVC_OPT_CAND_LOG": gvc_native.OPT_CAND_LOG}
+    assert opts == py
